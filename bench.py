@@ -1,0 +1,367 @@
+"""Benchmark of the B200 Block-Equivalence labeler; prints ONE JSON line (rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload 2d8192|2d2048|3d512|batch]
+
+Default workload (2d8192): 2D 8192x8192 uint8 images of the seven seeded families (Bernoulli
+p = 0.1 / 0.4 / 0.6 / 0.9, 2000 disks over p = 0.05 noise, serpentine, spiral), 8-connectivity,
+int32 labels.  One step labels one image (the families in turn), inputs resident in HBM.  The
+inputs (64 MiB) fit in L2, so a 512 MiB buffer is written between timed steps (L2 flush) and each
+step is timed alone with CUDA events on the labeling stream.
+
+`value` is Gpx/s over the timed steps (max over ranks for N > 1; every rank labels its own
+images, weak scaling).  `e2e` is the same metric through the host-buffer C-ABI call
+(be_label2d_host: pinned host image -> device -> labels -> pinned host labels, wall clock).
+`roofline` takes the algorithmic 5 bytes per pixel (1 B read + 4 B label write) of the whole
+labeling over the device time of its launches; `roofline_kernels` splits it per launch.
+`cpu_baseline` times the reference's own CPU labeler (compiled from its sources into
+oracle/_ref) on the host cores, on a bounded sample.
+
+--impl reference runs only that reference CPU labeler (all host threads) on the same workload
+and prints the same line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+STAGES_2D = ["k_tile_local_2d", "k_merge_2d", "k_post_2d", "k_segscan", "k_tile_write_2d"]
+STAGES_3D = ["k_tile_local_3d", "k_merge_3d", "k_post_3d", "k_segscan", "k_tile_write_3d"]
+# Algorithmic bytes per pixel of each launch (what the launch must move at minimum):
+# tile_local reads the image (1 B), tile_write writes the labels (4 B); the others move only
+# per-tile / per-segment metadata and have no per-pixel algorithmic traffic.
+ALGO_BYTES = {"k_tile_local_2d": 1.0, "k_tile_write_2d": 4.0, "k_tile_local_3d": 1.0,
+              "k_tile_write_3d": 4.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------
+# Workloads
+# ------------------------------------------------------------------------------------------
+
+def make_2d_inputs(side: int, families, seed: int):
+    from labeling_b200 import workloads as W
+    return [(f, W.family_8192(f, seed=seed + i, side=side)) for i, f in enumerate(families)]
+
+
+def make_3d_inputs(side: int, seed: int):
+    from labeling_b200 import workloads as W
+    out = []
+    for i, p in enumerate([0.1, 0.3, 0.5]):
+        out.append((f"bern{p}", W.bernoulli((side, side, side), p, seed + i)))
+    for pct in (50, 80):
+        out.append((f"grf{pct}", W.grf((side, side, side), 4.0, pct, seed + pct, device="cuda")))
+    return out
+
+
+# ------------------------------------------------------------------------------------------
+# Reference CPU labelers (oracle/_ref), bounded samples
+# ------------------------------------------------------------------------------------------
+
+def cpu_reference_2d(images, budget_s: float):
+    """Times the reference's CPU labeler on whole images until budget_s is spent.  Prefers the
+    reference's OpenMP block-equivalence labeler (bleq CPU) and falls back to its Grana labeler."""
+    from oracle import oracle as O
+    kind_name = None
+    fn = None
+    if hasattr(O, "ref_cpu_bleq") and O.cpu_lib() is not None:
+        fn, kind_name = O.ref_cpu_bleq, "reference bleq CPU (TLabelEquivalenceX2, OpenMP)"
+        cores = os.cpu_count() or 1
+    elif O.grana_lib() is not None:
+        fn, kind_name = (lambda im: O.ref_grana(im)), "reference gr-block CPU (Grana, 1 thread)"
+        cores = 1
+    else:
+        return None
+    px, t_total, n = 0, 0.0, 0
+    t_start = time.perf_counter()
+    i = 0
+    while True:
+        name, img = images[i % len(images)]
+        t0 = time.perf_counter()
+        fn(img)
+        t_total += time.perf_counter() - t0
+        px += img.size
+        n += 1
+        i += 1
+        if time.perf_counter() - t_start > budget_s and n >= min(len(images), 2):
+            break
+        if n >= 3 * len(images):
+            break
+    return {"value": px / t_total / 1e9, "unit": "Gpx/s", "cores": cores,
+            "kind": "reference", "sample": f"{n} whole images ({kind_name}), {t_total:.2f} s"}
+
+
+# ------------------------------------------------------------------------------------------
+# Our arm
+# ------------------------------------------------------------------------------------------
+
+def bench_ours(args, rank, world, local_rank):
+    import torch
+    import labeling_b200 as be
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    is3d = args.workload == "3d512"
+    if is3d:
+        inputs = make_3d_inputs(512, seed=100 + 17 * rank)
+        stages = STAGES_3D
+        metric, unit = "Gvox/s labeled (3D 512^3 BE, 26-conn)", "Gvox/s"
+    else:
+        side = 2048 if args.workload == "2d2048" else 8192
+        fams = ["bern0.5"] if side == 2048 else None
+        from labeling_b200 import workloads as W
+        inputs = make_2d_inputs(side, fams or W.FAMILIES_8192, seed=10 + 17 * rank)
+        stages = STAGES_2D
+        metric, unit = f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "Gpx/s"
+
+    ctx = be.Context(local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    d_in = [torch.from_numpy(a).to(dev) for _, a in inputs]
+    d_out = [torch.empty(a.shape, dtype=torch.int32, device=dev) for _, a in inputs]
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    npx = [a.size for _, a in inputs]
+
+    def label(i, want=False):
+        if is3d:
+            return be.label3d(ctx, d_in[i], d_out[i], want_count=want, stream=stream)
+        return be.label2d(ctx, d_in[i], d_out[i], want_count=want, stream=stream)
+
+    with torch.cuda.stream(stream):
+        for i in range(max(args.warmup, 3)):
+            label(i % len(inputs))
+        stream.synchronize()
+        counts = [label(i, want=True) for i in range(len(inputs))]
+
+        ctx.set_stage_timing(True)
+        ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        stage_ms = np.zeros(len(stages))
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        px_done = 0
+        with ClockSampler(local_rank) as clk:
+            for s in range(args.steps):
+                i = s % len(inputs)
+                flush.fill_(s & 0xFF)
+                ev0[s].record(stream)
+                label(i)
+                ev1[s].record(stream)
+                st = ctx.stage_times()
+                stage_ms += np.array(st[:len(stages)])
+                px_done += npx[i]
+            torch.cuda.synchronize()
+        ctx.set_stage_timing(False)
+        step_ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
+    t_ms = float(sum(step_ms))
+    if world > 1:
+        tt = torch.tensor([t_ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_ms = float(tt.item())
+        pp = torch.tensor([float(px_done)], device=dev)
+        torch.distributed.all_reduce(pp, op=torch.distributed.ReduceOp.SUM)
+        px_total = float(pp.item())
+    else:
+        px_total = float(px_done)
+    value = px_total / (t_ms / 1e3) / 1e9
+
+    # End to end through the host-buffer C-ABI call, pinned host memory.
+    h_in = [torch.from_numpy(a).pin_memory() for _, a in inputs]
+    h_out = [torch.empty(a.shape, dtype=torch.int32).pin_memory() for _, a in inputs]
+    for i in range(min(2, len(inputs))):
+        (be.label3d_host if is3d else be.label2d_host)(ctx, h_in[i].numpy(), out=h_out[i].numpy())
+    t0 = time.perf_counter()
+    e2e_px = 0
+    e2e_steps = max(1, min(args.steps, 2 * len(inputs)))
+    h2d = d2h = 0
+    for s in range(e2e_steps):
+        i = s % len(inputs)
+        (be.label3d_host if is3d else be.label2d_host)(ctx, h_in[i].numpy(), out=h_out[i].numpy())
+        e2e_px += npx[i]
+        h2d += npx[i]
+        d2h += 4 * npx[i] + 8
+    e2e_s = time.perf_counter() - t0
+    e2e = {"value": e2e_px / e2e_s / 1e9, "unit": unit, "h2d_bytes_per_step": int(h2d / e2e_steps),
+           "d2h_bytes_per_step": int(d2h / e2e_steps)}
+
+    peak, peak_kind = load_peaks()
+    steps = args.steps
+    pipe_ms = float(stage_ms.sum()) / steps
+    px_step = px_done / steps
+    achieved = 5.0 * px_step / (pipe_ms / 1e3) / 1e9
+    kernels = []
+    for name, ms in zip(stages, stage_ms / steps):
+        ab = ALGO_BYTES.get(name, 0.0) * px_step
+        kernels.append({"kernel": name, "ms": round(float(ms), 4),
+                        "share": round(float(ms) / pipe_ms, 4) if pipe_ms else None,
+                        "algorithmic_bytes": int(ab),
+                        "achieved_gbs": round(ab / (ms / 1e3) / 1e9, 1) if ab and ms else None})
+    dom = max(kernels, key=lambda k: k["ms"])
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(args.workload)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "peak_kind": peak_kind, "scope": "whole labeling (5 launches), 5 B/px",
+                "dominant_kernel": dom["kernel"],
+                "frac_of_8tbs": round(achieved / 8000.0, 4)}
+    clocks = clk.summary()
+
+    result = {
+        "metric": metric, "value": round(value, 3), "unit": unit, "n_gpus": world,
+        "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": round(t_ms / steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "images": [n for n, _ in inputs],
+                   "shape": list(inputs[0][1].shape), "connectivity": 26 if is3d else 8,
+                   "labels": "int32 canonical", "l2": "flushed between steps (512 MiB write)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": e2e, "roofline": roofline, "roofline_kernels": kernels,
+        "gpu_launches": 5 * steps, "clocks": clocks,
+        "components": {n: c for (n, _), c in zip(inputs, counts)},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        budget = 20.0
+        if is3d:
+            result["cpu_baseline"] = None
+        else:
+            result["cpu_baseline"] = cpu_reference_2d(inputs, budget)
+    ctx.close()
+    return result
+
+
+def bench_reference(args, rank, world):
+    if rank != 0:
+        return None
+    if args.workload == "3d512":
+        return {"impl": "reference", "unavailable": "the reference has no CPU 3D labeler (main.cpp:106,120,125)"}
+    side = 2048 if args.workload == "2d2048" else 8192
+    from labeling_b200 import workloads as W
+    fams = ["bern0.5"] if side == 2048 else W.FAMILIES_8192
+    inputs = make_2d_inputs(side, fams, seed=10)
+    for _ in range(max(0, min(args.warmup, 1))):
+        pass
+    cb = cpu_reference_2d(inputs, budget_s=30.0)
+    if cb is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}
+    return {"impl": "reference", "metric": f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "value": round(cb["value"], 4),
+            "unit": "Gpx/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded)", "config": {"workload": args.workload, "images": fams},
+            "cpu_baseline": cb, "e2e": {"value": round(cb["value"], 4), "unit": "Gpx/s",
+                                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=28)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="2d8192", choices=["2d8192", "2d2048", "3d512"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        res = bench_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = bench_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,108 @@
+/*
+ * be.h -- C ABI of the B200 Block-Equivalence (BE) connected-component labeler.
+ *
+ * Plain C: pointers, sizes and int status codes only.  Every entry point returns BE_OK (0) or a
+ * positive be_status; be_last_error() gives the message of the last failure on a context.
+ *
+ * Labels.  Output labels are int32, 0 = background, components numbered 1..K in the order of
+ * their first foreground pixel (voxel) in raster order (row-major; for volumes the last dimension
+ * is the fastest).  This is the reference BE result after canonical relabeling: the reference's
+ * own label values (1 + smallest block index in its padded block grid) differ only by a
+ * renumbering.  Foreground is `pixel > threshold`; threshold 0 reproduces the reference kernels'
+ * `pixel != 0` test and threshold 8 the binarization of ILabeling::RGB2Gray
+ * (Labeling2015/src/LabelingTools.cpp:39-49).
+ *
+ * Connectivity.  2D: 8-connectivity with 2x2 blocks (reference LBEQ2_*, LabelingAlgs.cl:136-319).
+ * 3D: 26-connectivity with 2x2x2 blocks (reference BLEQ3D_*, LabelingAlgs.cl:740-979).
+ *
+ * Threading.  A context is used by one host thread at a time.  Device buffers are owned by the
+ * caller; the context owns and reuses its scratch.  `stream` is a cudaStream_t (NULL = the legacy
+ * default stream).  Calls return once the work is enqueued, except where a host result is asked
+ * for (n_components != NULL, the *_host variants), which synchronize the stream.
+ */
+#ifndef BE_B200_H_
+#define BE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum be_status {
+    BE_OK = 0,
+    BE_ERR_INVALID = 1,        /* bad argument (null pointer, size, pitch, unsupported mode) */
+    BE_ERR_OOM = 2,            /* device or pinned host allocation failed */
+    BE_ERR_NO_CONVERGENCE = 3, /* iterative merge hit its iteration cap */
+    BE_ERR_CUDA = 4,           /* a CUDA call failed; see be_last_error */
+    BE_ERR_TIMEOUT = 5,        /* a bounded wait ran out (server / batch) */
+    BE_ERR_BUSY = 6,           /* admission refused: not enough free device memory or slots */
+    BE_ERR_CANCELLED = 7       /* the request was cancelled before it completed */
+} be_status;
+
+/* Merge algorithm. */
+enum {
+    BE_ALGO_AUTO = 0, /* the autotuned choice (union-find unless the tuner measured otherwise) */
+    BE_ALGO_UF = 1,   /* tile union-find in shared memory + global border merge */
+    BE_ALGO_ITER = 2  /* the paper's iterative scan / analyze, with a device-side change flag */
+};
+
+/* Connectivity selector, as the reference's TCoherence (LabelingTools.hpp:45-50). */
+enum { BE_COH_4 = 0, BE_COH_8 = 1, BE_COH_DEFAULT = 2 };
+
+typedef struct be_ctx be_ctx;
+
+/* Library version string ("major.minor.patch"). */
+const char *be_version(void);
+
+/* Context on CUDA device `device`.  Replaces IOCLLabeling::Init / InitOpenCL
+ * (LabelingTools.cpp:81-94, CLUtils.c:88-233): no runtime compilation, kernels are built in. */
+int be_create(be_ctx **ctx, int device);
+int be_destroy(be_ctx *ctx);
+/* Message of the last failed call on ctx (empty string when none). */
+const char *be_last_error(const be_ctx *ctx);
+
+/* 2D labeling of a device image.  Replaces TOCLLabelEquivalenceX2::DoOCLLabel
+ * (LabelingAlgs.cpp:1067-1084, kernels LabelingAlgs.cl:176-319) minus its padding: any
+ * rows x cols works, rows >= 1, cols >= 1, rows * cols < 2^31.
+ *   in       uint8 pixels, in_pitch bytes per row (>= cols)
+ *   out      int32 labels, out_pitch elements per row (>= cols); every pixel is written
+ *   coh      BE_COH_8 or BE_COH_DEFAULT (8-connectivity); BE_COH_4 is rejected like the
+ *            reference (LabelingAlgs.cpp:1070)
+ *   n_components  if not NULL: receives K (synchronizes `stream`)
+ */
+int be_label2d(be_ctx *ctx, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols,
+               int threshold, int coh, int algo, int32_t *out, int64_t out_pitch,
+               int64_t *n_components, void *stream);
+
+/* 3D labeling of a dense device volume [d0][d1][d2] (d2 fastest).  Replaces
+ * TOCLBlockEquivalence3D::DoOCLLabel3D (LabelingAlgs.cpp:1520-1536, kernels
+ * LabelingAlgs.cl:805-979) minus the padding; d0 * d1 * d2 < 2^31.  Output is the unpadded
+ * volume (the reference returns its padded copy, LabelingTools.cpp:217-220). */
+int be_label3d(be_ctx *ctx, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int threshold,
+               int algo, int32_t *out, int64_t *n_components, void *stream);
+
+/* Host-buffer variants: copy in through pinned staging, label, copy out, synchronize.  The
+ * equivalent of IOCLLabeling::Label / IOCLLabeling3D::Label (LabelingTools.cpp:98-132, 180-221)
+ * around the device call.  elapsed_us (optional) receives the device time of the labeling alone,
+ * measured with CUDA events (the reference's watch_ scope). */
+int be_label2d_host(be_ctx *ctx, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols,
+                    int threshold, int coh, int algo, int32_t *out, int64_t out_pitch,
+                    int64_t *n_components, double *elapsed_us);
+int be_label3d_host(be_ctx *ctx, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
+                    int threshold, int algo, int32_t *out, int64_t *n_components,
+                    double *elapsed_us);
+
+/* Per-launch timing of plain calls (no counterpart in the reference, whose stopwatch covers the
+ * whole DoOCLLabel call, LabelingTools.cpp:118-125).  When enabled, be_label2d / be_label3d
+ * record a CUDA event before and after each of their launches; be_stage_times then returns the
+ * device time of each launch of the last call in ms (it waits for that call's last event). */
+int be_set_stage_timing(be_ctx *ctx, int enable);
+int be_stage_times(be_ctx *ctx, float *ms, int max_stages, int *n_stages);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BE_B200_H_ */

@@ -1,0 +1,254 @@
+"""B200-native Block-Equivalence connected-component labeling.
+
+Python access to ``libbe_b200.so`` (the CUDA kernels behind the C ABI of ``include/be.h``)
+through ctypes, plus a mirror of the reference's labeler interface:
+
+* :class:`Context` -- one CUDA context's labeler state (``be_create`` / ``be_destroy``).
+* :func:`label2d` / :func:`label3d` -- device buffers (torch CUDA tensors or raw pointers) in,
+  int32 canonical labels out (``be_label2d`` / ``be_label3d``).
+* :func:`label2d_host` / :func:`label3d_host` -- numpy in, numpy out.
+* :class:`Labeling` / :class:`Labeling3D` -- ``Label(pixels, threads, coh) -> (labels, µs)``, the
+  shape of ``ILabeling::Label`` (Labeling2015/src/LabelingTools.hpp:58-73), selected through
+  :func:`make_labeler` with the reference's algorithm names (``bleq``, ``lbeq``).
+
+There is no CPU fallback: if the library is missing or no GPU is present, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbe_b200.so")
+
+BE_OK = 0
+STATUS = {0: "BE_OK", 1: "BE_ERR_INVALID", 2: "BE_ERR_OOM", 3: "BE_ERR_NO_CONVERGENCE",
+          4: "BE_ERR_CUDA", 5: "BE_ERR_TIMEOUT", 6: "BE_ERR_BUSY", 7: "BE_ERR_CANCELLED"}
+ALGO_AUTO, ALGO_UF, ALGO_ITER = 0, 1, 2
+COH_4, COH_8, COH_DEFAULT = 0, 1, 2
+
+_lib = None
+
+
+class BEError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C-ABI library (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m labeling_b200.build`")
+    l = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64, c_int = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_int
+    p64 = ctypes.POINTER(ctypes.c_int64)
+    pdbl = ctypes.POINTER(ctypes.c_double)
+    l.be_version.restype = ctypes.c_char_p
+    l.be_create.argtypes = [ctypes.POINTER(vp), c_int]
+    l.be_destroy.argtypes = [vp]
+    l.be_last_error.argtypes = [vp]
+    l.be_last_error.restype = ctypes.c_char_p
+    l.be_label2d.argtypes = [vp, vp, i64, i32, i32, c_int, c_int, c_int, vp, i64, p64, vp]
+    l.be_label3d.argtypes = [vp, vp, i32, i32, i32, c_int, c_int, vp, p64, vp]
+    l.be_label2d_host.argtypes = [vp, vp, i64, i32, i32, c_int, c_int, c_int, vp, i64, p64, pdbl]
+    l.be_label3d_host.argtypes = [vp, vp, i32, i32, i32, c_int, c_int, vp, p64, pdbl]
+    l.be_set_stage_timing.argtypes = [vp, c_int]
+    l.be_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), c_int, ctypes.POINTER(c_int)]
+    _lib = l
+    return l
+
+
+def version() -> str:
+    return lib().be_version().decode()
+
+
+class Context:
+    """Labeler state on one CUDA device; not thread-safe (one per host thread)."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        rc = lib().be_create(ctypes.byref(self._h), int(device))
+        if rc:
+            raise BEError(rc, f"be_create(device={device}) failed")
+        self.device = device
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if not self._h:
+            raise RuntimeError("context is closed")
+        return self._h
+
+    def check(self, rc: int) -> None:
+        if rc:
+            raise BEError(rc, lib().be_last_error(self._h).decode())
+
+    def set_stage_timing(self, on: bool) -> None:
+        self.check(lib().be_set_stage_timing(self.handle, int(on)))
+
+    def stage_times(self):
+        """Device ms of each launch of the last plain call (stage timing must be on)."""
+        ms = (ctypes.c_float * 16)()
+        n = ctypes.c_int(0)
+        self.check(lib().be_stage_times(self.handle, ms, 16, ctypes.byref(n)))
+        return [float(ms[i]) for i in range(n.value)]
+
+    def close(self) -> None:
+        if self._h:
+            lib().be_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ptr(x) -> int:
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    return int(x)
+
+
+def _stream(stream) -> Optional[int]:
+    if stream is None:
+        try:
+            import torch
+            return int(torch.cuda.current_stream().cuda_stream)
+        except Exception:
+            return None
+    if hasattr(stream, "cuda_stream"):
+        return int(stream.cuda_stream)
+    return int(stream)
+
+
+def label2d(ctx: Context, img, out, threshold: int = 0, algo: int = ALGO_AUTO,
+            coh: int = COH_DEFAULT, want_count: bool = True, stream=None,
+            in_pitch: Optional[int] = None, out_pitch: Optional[int] = None,
+            rows: Optional[int] = None, cols: Optional[int] = None) -> Optional[int]:
+    """Labels a device image.  ``img``: uint8 CUDA tensor [rows, cols] (or a pointer with
+    rows/cols/in_pitch); ``out``: int32 CUDA tensor of the same shape.  Returns the component
+    count (synchronizing) when ``want_count``."""
+    if hasattr(img, "shape"):
+        rows, cols = int(img.shape[0]), int(img.shape[1])
+        in_pitch = int(img.stride(0)) if in_pitch is None else in_pitch
+        out_pitch = int(out.stride(0)) if out_pitch is None else out_pitch
+    n = ctypes.c_int64(0)
+    ctx.check(lib().be_label2d(ctx.handle, _ptr(img), in_pitch, rows, cols, threshold, coh, algo,
+                               _ptr(out), out_pitch, ctypes.byref(n) if want_count else None,
+                               _stream(stream)))
+    return int(n.value) if want_count else None
+
+
+def label3d(ctx: Context, vol, out, threshold: int = 0, algo: int = ALGO_AUTO,
+            want_count: bool = True, stream=None, dims=None) -> Optional[int]:
+    """Labels a dense device volume [d0, d1, d2] (d2 fastest) into int32 ``out``."""
+    d0, d1, d2 = (int(s) for s in (vol.shape if dims is None else dims))
+    n = ctypes.c_int64(0)
+    ctx.check(lib().be_label3d(ctx.handle, _ptr(vol), d0, d1, d2, threshold, algo, _ptr(out),
+                               ctypes.byref(n) if want_count else None, _stream(stream)))
+    return int(n.value) if want_count else None
+
+
+def label2d_host(ctx: Context, img: np.ndarray, threshold: int = 0, algo: int = ALGO_AUTO,
+                 coh: int = COH_DEFAULT, out: Optional[np.ndarray] = None) -> Tuple[np.ndarray, int, float]:
+    """numpy uint8 [rows, cols] -> (int32 labels, component count, device µs).  Pass page-locked
+    arrays (e.g. numpy views of pinned torch tensors) for full-speed copies."""
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    rows, cols = img.shape
+    if out is None:
+        out = np.empty((rows, cols), np.int32)
+    assert out.shape == (rows, cols) and out.dtype == np.int32 and out.flags.c_contiguous
+    n, us = ctypes.c_int64(0), ctypes.c_double(0)
+    ctx.check(lib().be_label2d_host(ctx.handle, img.ctypes.data, cols, rows, cols, threshold, coh,
+                                    algo, out.ctypes.data, cols, ctypes.byref(n), ctypes.byref(us)))
+    return out, int(n.value), float(us.value)
+
+
+def label3d_host(ctx: Context, vol: np.ndarray, threshold: int = 0, algo: int = ALGO_AUTO,
+                 out: Optional[np.ndarray] = None) -> Tuple[np.ndarray, int, float]:
+    vol = np.ascontiguousarray(vol, dtype=np.uint8)
+    if out is None:
+        out = np.empty(vol.shape, np.int32)
+    assert out.shape == vol.shape and out.dtype == np.int32 and out.flags.c_contiguous
+    n, us = ctypes.c_int64(0), ctypes.c_double(0)
+    ctx.check(lib().be_label3d_host(ctx.handle, vol.ctypes.data, *vol.shape, threshold, algo,
+                                    out.ctypes.data, ctypes.byref(n), ctypes.byref(us)))
+    return out, int(n.value), float(us.value)
+
+
+# --- the reference's labeler interface (ILabeling / IOCLLabeling3D shape) --------------------
+
+class Labeling:
+    """2D labeler with the call shape of ``ILabeling::Label``: binarizes with threshold 8 (the
+    reference's ``RGB2Gray``, LabelingTools.cpp:39-49), labels on the GPU and returns
+    ``(labels, time_us)``; ``time_us`` covers the labeling only, like the reference's ``watch_``.
+    ``threads`` is accepted for interface parity and ignored (OpenMP thread count)."""
+
+    threshold = 8
+
+    def __init__(self, algo: int = ALGO_AUTO, device: int = 0):
+        self.ctx = Context(device)
+        self.algo = algo
+
+    def Label(self, pixels: np.ndarray, threads: int = 0, coh: int = COH_DEFAULT):
+        if pixels.size == 0:
+            raise ValueError("Labeling.Label : Input image is empty")
+        if pixels.ndim == 3:   # colour input: cv::cvtColor(COLOR_RGB2GRAY) weights
+            pixels = np.rint(pixels[..., 0] * 0.299 + pixels[..., 1] * 0.587 +
+                             pixels[..., 2] * 0.114).astype(np.uint8)
+        labels, _, us = label2d_host(self.ctx, pixels, self.threshold, self.algo, coh)
+        return labels, us
+
+
+class Labeling3D:
+    """3D labeler with the call shape of ``IOCLLabeling3D::Label`` (LabelingTools.cpp:180-221):
+    only the default connectivity is accepted; the input volume is used as is (``Read3DImage``
+    already binarized its slices)."""
+
+    threshold = 0
+
+    def __init__(self, algo: int = ALGO_AUTO, device: int = 0):
+        self.ctx = Context(device)
+        self.algo = algo
+
+    def Label(self, pixels: np.ndarray, threads: int = 0, coh: int = COH_DEFAULT):
+        if pixels.size == 0:
+            raise ValueError("Labeling3D.Label : Input image is empty")
+        if pixels.ndim != 3:
+            raise ValueError("Labeling3D.Label : Input image is not a 3D image")
+        if coh != COH_DEFAULT:
+            raise ValueError("Labeling3D.Label : Only default coherence is supported for 3D labeling")
+        labels, _, us = label3d_host(self.ctx, pixels, self.threshold, self.algo)
+        return labels, us
+
+
+ALGORITHMS = {
+    "bleq": ("Block equivalence by Zavalishin et.al. 2016", ALGO_AUTO),
+    "lbeq": ("Label equivalence (iterative scan/analyze form)", ALGO_ITER),
+}
+
+
+def make_labeler(name: str, gpu: bool = True, three_d: bool = False, device: int = 0):
+    """The reference's algorithm registry (main.cpp:101-131, SetLabelingAlg :373-395) for the GPU
+    slots this package fills: ``-a bleq|lbeq [-3] -g``.  CPU slots are not provided."""
+    if name not in ALGORITHMS:
+        raise ValueError("No labeling algorithm specified" if not name else
+                         f"Chosen algorithm '{name}' is not provided by the GPU labeler")
+    if not gpu:
+        raise ValueError("Chosen algorithm doesn't support specified capabilities (CPU mode)")
+    algo = ALGORITHMS[name][1]
+    return Labeling3D(algo, device) if three_d else Labeling(algo, device)

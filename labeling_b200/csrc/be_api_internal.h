@@ -1,0 +1,76 @@
+// be_api_internal.h -- host-side state behind the C ABI (not part of the public interface).
+#pragma once
+#include "be_common.cuh"
+
+#include <cuda_runtime.h>
+#include <string>
+
+namespace be {
+
+constexpr int kQueueWords = 16;   // work-queue counters per workspace (one per kernel)
+
+// Per-tile sizes of a pipeline's workspace.
+struct Geometry {
+    size_t lab_bytes_per_tile;
+    int nperim;
+    int maxb;
+};
+
+Geometry geometry_2d();
+Geometry geometry_3d();
+size_t layout_work(const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_imgs, char *base, Work *w);
+
+// One growable device allocation holding a Work.
+struct Workspace {
+    void *base = nullptr;
+    size_t bytes = 0;
+    int64_t cap_tiles = 0, cap_segs = 0;
+    int cap_imgs = 0;
+    Work w{};
+    int ensure(struct ::be_ctx *ctx, const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_imgs);
+    void release();
+};
+
+// Scratch of the iterative (scan / analyze) form.
+struct IterWork {
+    void *base = nullptr;
+    size_t bytes = 0;
+};
+
+int set_error(struct ::be_ctx *ctx, int code, const char *fmt, ...);
+int cuda_error(struct ::be_ctx *ctx, cudaError_t e, const char *what);
+
+void fill_img2d(Img2D &im, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols, int thr,
+                int32_t *out, int64_t out_pitch, int64_t tile_base, int64_t seg_base, int index);
+void fill_img3d(Img3D &im, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int thr,
+                int32_t *out, int64_t tile_base, int64_t seg_base, int index);
+constexpr int kStages = 5;   // launches of one union-find pipeline
+cudaError_t launch_uf2d(const ImgList2D &L, const Work &w, int sms, bool persistent, cudaStream_t s,
+                        cudaEvent_t *ev = nullptr);
+cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persistent, cudaStream_t s,
+                        cudaEvent_t *ev = nullptr);
+
+int run_iter2d(struct ::be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols,
+               int thr, int32_t *out, int64_t out_pitch, cudaStream_t s);
+int run_iter3d(struct ::be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int thr,
+               int32_t *out, cudaStream_t s);
+
+}  // namespace be
+
+struct be_ctx {
+    int device = 0;
+    int sms = 148;
+    std::string err;
+    be::Workspace ws2d, ws3d, wsiter;
+    void *iter_base = nullptr;      // iterative-form block arrays
+    size_t iter_bytes = 0;
+    uint32_t *iter_err = nullptr;   // pinned: iteration-cap flag of the last iterative call
+    void *d_in = nullptr, *d_out = nullptr;   // device staging of the *_host calls
+    size_t d_in_bytes = 0, d_out_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t *h_ncomp = nullptr;     // pinned
+    bool timing = false;            // record an event between the launches of a plain call
+    int timed_stages = 0;
+    cudaEvent_t stage_ev[be::kStages + 1] = {};
+};

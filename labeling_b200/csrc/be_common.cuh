@@ -1,0 +1,252 @@
+// be_common.cuh -- shared device code for the B200 Block-Equivalence labeler.
+//
+// Terminology (follows the reference's BE method, LabelingAlgs.cl:133-319 / 737-979):
+//   block      2x2 pixels (2D) or 2x2x2 voxels (3D); the reference's "super pixel".
+//   mask       which pixels/voxels of a block are foreground (4 / 8 bits).
+//   tile       the rectangle (box) of blocks one CTA labels in shared memory.
+//   key        the raster index of a pixel/voxel inside its image (row-major, last dim fastest).
+//              A component is represented by its smallest key (its first pixel in raster order);
+//              that is what makes the output canonical.
+//   node       a tile-local component that touches the tile border; nodes are merged across
+//              tiles with a global union-find.
+//   segment    the part of one image row (a line along the fastest dimension) that lies in one
+//              tile; per-segment root counts give each component its canonical rank.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace be {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// ---------------------------------------------------------------------------------------------
+// Image descriptors.  One pipeline launch labels a list of images (the plain API passes one).
+// ---------------------------------------------------------------------------------------------
+struct Img2D {
+    const uint8_t *in;   // row-major uint8, in_pitch bytes per row
+    int32_t *out;        // row-major int32 labels, out_pitch elements per row
+    int64_t in_pitch;
+    int64_t out_pitch;
+    int32_t rows, cols;
+    int32_t tiles_x, tiles_y;
+    int64_t tile_base;   // index of the image's first tile in the launch
+    int64_t seg_base;    // index of the image's first segment in the launch
+    int32_t thr;         // foreground is pixel > thr
+    int32_t index;       // position in the caller's list (for per-image outputs)
+};
+
+struct Img3D {
+    const uint8_t *in;   // dense [d0][d1][d2] uint8, d2 fastest
+    int32_t *out;        // dense [d0][d1][d2] int32 labels
+    int32_t d0, d1, d2;
+    int32_t t0, t1, t2;  // tile counts per dimension
+    int64_t tile_base;
+    int64_t seg_base;
+    int32_t thr;
+    int32_t index;
+};
+
+// The images of one launch: a device array, or a single descriptor passed by value (plain calls
+// need no descriptor upload).
+template <class Img>
+struct ImgList {
+    const Img *ptr;
+    int n;
+    Img one;
+    __device__ __forceinline__ Img get(int64_t tile) const;
+};
+
+// Global scratch of one pipeline launch ("workspace").  Sizes are per tile so that every tile
+// owns fixed-size slices and no kernel needs a prefix sum to find its data.
+struct Work {
+    void *lab;            // per-block tile-local labels: uint16 (2D) / uint32 (3D), NBLK per tile
+    uint16_t *perim;      // per tile NPERIM border entries: (node << 4) | side bits, 0 = empty
+    uint32_t *nb;         // per tile: number of nodes
+    uint32_t *gp;         // per node (tile * MAXB + j): union-find parent (global node id)
+    uint32_t *nkey;       // per node: key of the node's root pixel
+    uint16_t *nlrank;     // per node: rank of the root among the tile's roots in its segment
+    uint16_t *nroot;      // per node: tile-local block index of the node's root block
+    uint32_t *grank;      // per node that stays a root: rank among global roots in its segment
+    uint8_t *segcnt;      // per segment: number of component roots (uint8, word-padded)
+    uint32_t *segpref;    // per segment + 1: exclusive prefix of segcnt over the launch
+    uint32_t *chunksum;   // per scan chunk: sum of segcnt
+    uint32_t *queue;      // work-queue counters (persistent mode); zeroed before a launch
+    int64_t *ncomp;       // per image: number of components
+    uint32_t *err;        // error flags (bounded waits / iteration caps)
+    int64_t n_tiles;
+    int64_t n_segs;
+    int32_t n_chunks;
+    int32_t n_imgs;
+};
+
+constexpr int kScanChunk = 16384;   // segments per scan chunk (one CTA)
+
+// ---------------------------------------------------------------------------------------------
+// Small helpers.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p)
+{
+    return *reinterpret_cast<const volatile uint32_t *>(p);
+}
+
+// Foreground bits of four packed pixels: bit k = byte k > thr.
+__device__ __forceinline__ uint32_t fg4(uint32_t w, uint32_t thr4)
+{
+    uint32_t m = __vcmpgtu4(w, thr4) & 0x01010101u;
+    return (m * 0x10204080u) >> 28;
+}
+
+// Foreground bits of 16 pixels held in a uint4 (bit k = pixel k).
+__device__ __forceinline__ uint32_t fg16(uint4 v, uint32_t thr4)
+{
+    return fg4(v.x, thr4) | (fg4(v.y, thr4) << 4) | (fg4(v.z, thr4) << 8) | (fg4(v.w, thr4) << 12);
+}
+
+// Spread the 8 bit-pairs of a 16-bit word into the low two bits of 8 nibbles.
+__device__ __forceinline__ uint32_t pairs_to_nibbles(uint32_t x)
+{
+    x &= 0xFFFFu;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    return x;
+}
+
+// Union-find find over a shared-memory parent array (parents never exceed their child).
+__device__ __forceinline__ uint32_t sfind(const uint32_t *P, uint32_t a)
+{
+    uint32_t p = P[a];
+    while (p != a) {
+        a = p;
+        p = P[a];
+    }
+    return a;
+}
+
+// Merge of two shared-memory union-find trees that keeps the smaller index as the root
+// (the atomicMin formulation of Playne & Hawick's union-find, safe under concurrent merges).
+__device__ __forceinline__ void smerge(uint32_t *P, uint32_t a, uint32_t b)
+{
+    for (;;) {
+        a = sfind(P, a);
+        b = sfind(P, b);
+        if (a == b) return;
+        if (a < b) {
+            uint32_t old = atomicMin(&P[b], a);
+            if (old == b) return;
+            b = old;
+        } else {
+            uint32_t old = atomicMin(&P[a], b);
+            if (old == a) return;
+            a = old;
+        }
+    }
+}
+
+// Global union-find find with path halving.  Only non-root entries are rewritten and only with an
+// ancestor, which stays correct while other threads link roots (roots change only by CAS).
+__device__ __forceinline__ uint32_t gfind(uint32_t *gp, uint32_t a)
+{
+    uint32_t p = ld_volatile(gp + a);
+    while (p != a) {
+        uint32_t g = ld_volatile(gp + p);
+        if (g != p) *reinterpret_cast<volatile uint32_t *>(gp + a) = g;
+        a = p;
+        p = g;
+    }
+    return a;
+}
+
+// Read-only find (after all merges of the launch are complete).
+__device__ __forceinline__ uint32_t gfind_ro(const uint32_t *gp, uint32_t a)
+{
+    uint32_t p = gp[a];
+    while (p != a) {
+        a = p;
+        p = gp[a];
+    }
+    return a;
+}
+
+// Decrement a uint8 counter packed in a 32-bit word (the counter is >= 1 when this is called).
+__device__ __forceinline__ void dec_u8(uint8_t *base, int64_t idx)
+{
+    uint32_t *w = reinterpret_cast<uint32_t *>(base + (idx & ~int64_t(3)));
+    atomicSub(w, 1u << (8 * (idx & 3)));
+}
+
+// Block-wide exclusive scan of one uint32 per thread; returns the thread's prefix and writes the
+// total to *total.  `tmp` must hold blockDim.x / 32 + 1 words.
+template <int NT>
+__device__ __forceinline__ uint32_t block_exscan(uint32_t v, uint32_t *tmp, uint32_t *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) tmp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = lane < NT / 32 ? tmp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < NT / 32) tmp[lane] = s;
+        if (lane == NT / 32 - 1) tmp[NT / 32] = s;
+    }
+    __syncthreads();
+    uint32_t r = x - v + (warp ? tmp[warp - 1] : 0);
+    *total = tmp[NT / 32];
+    __syncthreads();
+    return r;
+}
+
+// Index of the image that owns global item `t`, by binary search over the images' bases.
+template <class Img>
+__device__ __forceinline__ int find_img_tile(const Img *imgs, int n, int64_t t)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (imgs[mid].tile_base <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class Img>
+__device__ __forceinline__ Img ImgList<Img>::get(int64_t tile) const
+{
+    return n == 1 ? one : ptr[find_img_tile(ptr, n, tile)];
+}
+
+using ImgList2D = ImgList<Img2D>;
+using ImgList3D = ImgList<Img3D>;
+
+// Work distribution: with a queue counter every CTA pulls items until none are left (persistent
+// launch); without one, CTA b takes items b, b + grid, ...
+struct ItemLoop {
+    uint32_t *queue;
+    int64_t n;
+    __device__ __forceinline__ int64_t first(uint32_t *slot)
+    {
+        if (!queue) return blockIdx.x;
+        if (threadIdx.x == 0) *slot = atomicAdd(queue, 1u);
+        __syncthreads();
+        int64_t v = *slot;
+        __syncthreads();
+        return v;
+    }
+    __device__ __forceinline__ int64_t next(int64_t cur, uint32_t *slot)
+    {
+        if (!queue) return cur + gridDim.x;
+        return first(slot);
+    }
+};
+
+}  // namespace be

@@ -1,0 +1,39 @@
+// be_kernels.h -- kernel entry points and tile geometry shared by the host code (be_api.cu)
+// and the kernel files.
+#pragma once
+#include "be_common.cuh"
+
+// 2D tile: 128 x 32 blocks = 256 x 64 pixels.
+#define T2_TBW 128
+#define T2_TBH 32
+#define T2_NPERIM (2 * (T2_TBW + T2_TBH))
+#define T2_MAXB T2_NPERIM
+
+// 3D tile: 8 x 16 x 32 blocks = 16 x 32 x 64 voxels (d0, d1, d2).
+#define T3_TB0 8
+#define T3_TB1 16
+#define T3_TB2 32
+#define T3_NBLK (T3_TB0 * T3_TB1 * T3_TB2)
+#define T3_NPERIM (2 * (T3_TB0 * T3_TB1 + T3_TB0 * T3_TB2 + T3_TB1 * T3_TB2))
+#define T3_MAXB T3_NPERIM
+
+namespace be {
+
+__global__ void k_tile_local_2d(ImgList2D L, Work w);
+__global__ void k_merge_2d(ImgList2D L, Work w);
+__global__ void k_post_2d(ImgList2D L, Work w);
+__global__ void k_tile_write_2d(ImgList2D L, Work w);
+
+__global__ void k_tile_local_3d(ImgList3D L, Work w);
+__global__ void k_merge_3d(ImgList3D L, Work w);
+__global__ void k_post_3d(ImgList3D L, Work w);
+__global__ void k_tile_write_3d(ImgList3D L, Work w);
+
+__global__ void k_segscan(Work w);
+
+constexpr int kPostThreads = 128;
+constexpr int kT3Threads = 256;
+constexpr int kT3MergeThreads = 256;
+constexpr int kScanThreads = 256;
+
+}  // namespace be

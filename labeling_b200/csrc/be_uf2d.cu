@@ -1,0 +1,542 @@
+// be_uf2d.cu -- 2D Block-Equivalence labeling, union-find form (8-connectivity, 2x2 blocks).
+//
+// Replaces the reference's LBEQ2_Init / LBEQ2_Scan / LBEQ2_Analyze / LBEQ2_SetFinalLabels
+// (LabelingAlgs.cl:176-319) and their host loop (LabelingAlgs.cpp:989-1084) with five launches:
+//
+//   k_tile_local_2d   one CTA per 64x256-pixel tile: 16-byte coalesced loads, 2x2 block masks,
+//                     block union-find in shared memory (atomicMin, smaller key wins), flatten,
+//                     write one uint16 per block = (mask << 12) | tile-local root block; count
+//                     roots per segment; export border components as nodes.
+//   k_merge_2d        unions nodes across tile borders (global union-find, smaller key wins);
+//                     every root that gets linked is removed from its segment count.
+//   k_post            (be_scan.cu) ranks of surviving border roots + scan-chunk sums.
+//   k_segscan         (be_scan.cu) exclusive scan of the segment counts.
+//   k_tile_write_2d   one CTA per tile: resolves each block's canonical label and writes the int32
+//                     labels with 16-byte stores.
+//
+// Canonical numbering.  A block's key is the raster index of its first foreground pixel.  Blocks
+// are merged so that every component is rooted at its smallest key, i.e. at its first pixel in
+// raster order; its label is 1 + the number of component roots that precede that pixel.  The root
+// counts per segment (image row x tile column) and their exclusive prefix give that number.
+//
+// Shared-memory union-find slots.  Within a tile the union-find runs over "slots" whose order is
+// the key order: slot = r * 2*TBW + t * TBW + c for the block in block-row r, block-column c,
+// where t = 0 when the block has a foreground pixel in its top pixel row and 1 otherwise.  Its
+// first pixel is in pixel row 2r + t, so slot order equals raster order of first pixels, and the
+// atomicMin union keeps the first pixel's block as the root.
+#include "be_common.cuh"
+#include "be_kernels.h"
+#include "be_scan.cuh"
+
+namespace be {
+
+namespace {
+
+constexpr int TBW = T2_TBW, TBH = T2_TBH;          // tile in blocks
+constexpr int TW = 2 * TBW, TH = 2 * TBH;          // tile in pixels
+constexpr int NBLK = TBW * TBH;                    // blocks per tile (4096)
+constexpr int NPERIM = T2_NPERIM;                  // border positions per tile
+constexpr int MAXB = T2_MAXB;                      // nodes per tile
+constexpr int K1_NT = 256;
+constexpr int ITEMS = NBLK / 8;                    // 8-block row groups per tile
+constexpr int GROUPS = TBW / 8;                    // groups per block row
+
+static_assert(NBLK <= 4096, "tile-local block index must fit 12 bits");
+static_assert(MAXB < 4096, "node index must fit 12 bits");
+
+// Mask bits: 0 = top-left, 1 = top-right, 2 = bottom-left, 3 = bottom-right pixel.
+__device__ __forceinline__ uint32_t slot_of(int r, int c, uint32_t m)
+{
+    return uint32_t(r) * (2 * TBW) + ((m & 3u) ? 0u : uint32_t(TBW)) + uint32_t(c);
+}
+
+// Pixel offset (row, column) of a block's first foreground pixel, inside the block.
+__device__ __forceinline__ void first_px(uint32_t m, int &dy, int &dx)
+{
+    if (m & 3u) { dy = 0; dx = (m & 1u) ? 0 : 1; }
+    else { dy = 1; dx = (m & 4u) ? 0 : 1; }
+}
+
+__device__ __forceinline__ bool hconn(uint32_t left, uint32_t right)
+{
+    return (left & 0xAu) && (right & 0x5u);
+}
+
+// Block position of border position p of a tile with nbr x nbc valid blocks.
+__device__ __forceinline__ bool perim_pos(int p, int nbr, int nbc, int &r, int &c)
+{
+    if (p < TBW) { r = 0; c = p; return c < nbc; }
+    if (p < 2 * TBW) { r = nbr - 1; c = p - TBW; return c < nbc; }
+    if (p < 2 * TBW + TBH) { r = p - 2 * TBW; c = 0; return r < nbr; }
+    r = p - 2 * TBW - TBH; c = nbc - 1;
+    return r < nbr;
+}
+
+__device__ __forceinline__ uint32_t nib2byte(uint32_t x)
+{
+    x &= 0xFFFFu;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    return x;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Tile-local labeling.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(K1_NT) k_tile_local_2d(ImgList2D L, Work w)
+{
+    __shared__ uint32_t P[2 * NBLK];
+    __shared__ __align__(16) uint8_t M[NBLK];
+    __shared__ uint32_t RB[TH][TW / 32];
+    __shared__ uint32_t BF[NBLK / 32];
+    __shared__ uint32_t BP[NBLK / 32];
+    __shared__ uint32_t tmp[K1_NT / 32 + 1];
+    __shared__ uint32_t qslot;
+
+    const int tid = threadIdx.x;
+    uint16_t *lab = reinterpret_cast<uint16_t *>(w.lab);
+    ItemLoop loop{w.queue ? w.queue + 0 : nullptr, w.n_tiles};
+    for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
+        const Img2D im = L.get(t);
+        const int64_t lt = t - im.tile_base;
+        const int ty = int(lt / im.tiles_x), tx = int(lt - int64_t(ty) * im.tiles_x);
+        const int y0 = ty * TH, x0 = tx * TW;
+        const int nrp = min(TH, im.rows - y0), ncp = min(TW, im.cols - x0);
+        const int nbr = (nrp + 1) >> 1, nbc = (ncp + 1) >> 1;
+        const uint32_t thr4 = uint32_t(im.thr) * 0x01010101u;
+
+        for (int i = tid; i < TH * (TW / 32); i += K1_NT) (&RB[0][0])[i] = 0;
+        if (tid < NBLK / 32) BF[tid] = 0;
+
+        // Phase A: load pixels, build block masks, seed the union-find with horizontal runs.
+        uint32_t masks[ITEMS / K1_NT];
+#pragma unroll
+        for (int i = 0; i < ITEMS / K1_NT; ++i) {
+            const int it = tid + i * K1_NT, r = it / GROUPS, g = it % GROUPS;
+            uint32_t top = 0, bot = 0;
+            if (r < nbr && 16 * g < ncp) {
+                const int py = y0 + 2 * r, px = x0 + 16 * g;
+                const uint8_t *row0 = im.in + int64_t(py) * im.in_pitch + px;
+                const bool row1 = py + 1 < im.rows;
+                const bool vec = (16 * g + 16 <= ncp) &&
+                                 ((reinterpret_cast<uintptr_t>(row0) | uintptr_t(im.in_pitch)) & 15) == 0;
+                if (vec) {
+                    top = fg16(__ldg(reinterpret_cast<const uint4 *>(row0)), thr4);
+                    if (row1) bot = fg16(__ldg(reinterpret_cast<const uint4 *>(row0 + im.in_pitch)), thr4);
+                } else {
+                    const int n = min(16, ncp - 16 * g);
+                    for (int x = 0; x < n; ++x) {
+                        top |= uint32_t(row0[x] > im.thr) << x;
+                        if (row1) bot |= uint32_t(row0[im.in_pitch + x] > im.thr) << x;
+                    }
+                }
+            }
+            const uint32_t ms = pairs_to_nibbles(top) | (pairs_to_nibbles(bot) << 2);
+            masks[i] = ms;
+            *reinterpret_cast<uint2 *>(&M[r * TBW + 8 * g]) = make_uint2(nib2byte(ms), nib2byte(ms >> 16));
+            // Horizontal runs inside the group: every block points at the run's smallest slot.
+            uint32_t pm[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t m = (ms >> (4 * k)) & 15u;
+                const uint32_t s = slot_of(r, 8 * g + k, m);
+                const bool hc = k > 0 && hconn((ms >> (4 * (k - 1))) & 15u, m);
+                pm[k] = hc ? min(pm[k - 1], s) : s;
+            }
+            uint32_t run = 0;
+#pragma unroll
+            for (int k = 7; k >= 0; --k) {
+                const uint32_t m = (ms >> (4 * k)) & 15u;
+                if (!m) continue;
+                const bool last = (k == 7) || !hconn(m, (ms >> (4 * (k + 1))) & 15u);
+                if (last) run = pm[k];
+                P[slot_of(r, 8 * g + k, m)] = run;
+            }
+        }
+        __syncthreads();
+
+        // Phase B: merges with the block to the left (across groups) and the row above.
+#pragma unroll
+        for (int i = 0; i < ITEMS / K1_NT; ++i) {
+            const int it = tid + i * K1_NT, r = it / GROUPS, g = it % GROUPS;
+            const uint32_t ms = masks[i];
+            if (!ms) continue;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t m = (ms >> (4 * k)) & 15u;
+                if (!m) continue;
+                const int c = 8 * g + k;
+                const uint32_t s = slot_of(r, c, m);
+                const uint32_t ml = k > 0 ? (ms >> (4 * (k - 1))) & 15u : (c > 0 ? M[r * TBW + c - 1] : 0u);
+                const bool hcl = hconn(ml, m);
+                if (k == 0 && hcl) smerge(P, s, slot_of(r, c - 1, ml));
+                if (r == 0) continue;
+                const uint8_t *U = &M[(r - 1) * TBW];
+                const uint32_t up = U[c], upl = c > 0 ? U[c - 1] : 0u, upr = c + 1 < TBW ? U[c + 1] : 0u;
+                bool cN = (m & 3u) && (up & 0xCu);
+                bool cNW = (m & 1u) && (upl & 8u);
+                bool cNE = (m & 2u) && (upr & 4u);
+                if (hcl) {   // the left block is in this block's run and already covers these
+                    if ((ml & 3u) && (upl & 0xCu)) cNW = false;
+                    if ((ml & 2u) && (up & 4u)) cN = false;
+                }
+                if (cN) {    // upper blocks joined horizontally to `up` come with it
+                    if (hconn(upl, up)) cNW = false;
+                    if (hconn(up, upr)) cNE = false;
+                }
+                if (cN) smerge(P, s, slot_of(r - 1, c, up));
+                if (cNW) smerge(P, s, slot_of(r - 1, c - 1, upl));
+                if (cNE) smerge(P, s, slot_of(r - 1, c + 1, upr));
+            }
+        }
+        __syncthreads();
+
+        // Phase C: flatten, write tile-local labels, mark roots.
+#pragma unroll
+        for (int i = 0; i < ITEMS / K1_NT; ++i) {
+            const int it = tid + i * K1_NT, r = it / GROUPS, g = it % GROUPS;
+            const uint32_t ms = masks[i];
+            uint32_t e[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t m = (ms >> (4 * k)) & 15u;
+                e[k] = 0;
+                if (!m) continue;
+                const int c = 8 * g + k;
+                const uint32_t s = slot_of(r, c, m);
+                const uint32_t root = sfind(P, s);
+                P[s] = root;
+                const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
+                e[k] = (m << 12) | rb;
+                if (root == s) {
+                    int dy, dx;
+                    first_px(m, dy, dx);
+                    const int y = 2 * r + dy, x = 2 * c + dx;
+                    atomicOr(&RB[y][x >> 5], 1u << (x & 31));
+                }
+            }
+            uint4 v;
+            v.x = e[0] | (e[1] << 16); v.y = e[2] | (e[3] << 16);
+            v.z = e[4] | (e[5] << 16); v.w = e[6] | (e[7] << 16);
+            *reinterpret_cast<uint4 *>(lab + t * NBLK + r * TBW + 8 * g) = v;
+        }
+        __syncthreads();
+
+        // Phase D: segment counts, border components -> nodes.
+        if (tid < TH && tid < nrp) {
+            uint32_t cnt = 0;
+#pragma unroll
+            for (int k = 0; k < TW / 32; ++k) cnt += __popc(RB[tid][k]);
+            w.segcnt[im.seg_base + int64_t(y0 + tid) * im.tiles_x + tx] = uint8_t(cnt);
+        }
+        for (int p = tid; p < NPERIM; p += K1_NT) {
+            int r, c;
+            if (!perim_pos(p, nbr, nbc, r, c)) continue;
+            const uint32_t m = M[r * TBW + c];
+            if (!m) continue;
+            const uint32_t root = P[slot_of(r, c, m)];
+            const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
+            atomicOr(&BF[rb >> 5], 1u << (rb & 31));
+        }
+        __syncthreads();
+        uint32_t nb;
+        const uint32_t pre = block_exscan<K1_NT>(tid < NBLK / 32 ? __popc(BF[tid]) : 0u, tmp, &nb);
+        if (tid < NBLK / 32) BP[tid] = pre;
+        __syncthreads();
+        if (tid < NBLK / 32) {
+            uint32_t bits = BF[tid];
+            uint32_t j = pre;
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                const uint32_t rb = tid * 32 + b;
+                const uint32_t m = M[rb];
+                int dy, dx;
+                first_px(m, dy, dx);
+                const int rr = int(rb) / TBW, cc = int(rb) % TBW;
+                const int y = 2 * rr + dy, x = 2 * cc + dx;
+                uint32_t rank = __popc(RB[y][x >> 5] & ((1u << (x & 31)) - 1u));
+                for (int k = 0; k < (x >> 5); ++k) rank += __popc(RB[y][k]);
+                const int64_t node = t * MAXB + j;
+                w.nroot[node] = uint16_t(rb);
+                w.nkey[node] = uint32_t(int64_t(y0 + y) * im.cols + (x0 + x));
+                w.nlrank[node] = uint16_t(rank);
+                w.gp[node] = uint32_t(node);
+                ++j;
+            }
+        }
+        for (int p = tid; p < NPERIM; p += K1_NT) {
+            int r, c;
+            uint16_t ent = 0;
+            if (perim_pos(p, nbr, nbc, r, c)) {
+                const uint32_t m = M[r * TBW + c];
+                if (m) {
+                    const uint32_t root = P[slot_of(r, c, m)];
+                    const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
+                    const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
+                    ent = uint16_t((j << 4) | m);
+                }
+            }
+            w.perim[t * NPERIM + p] = ent;
+        }
+        if (tid == 0) w.nb[t] = nb;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Cross-tile merge.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ void link_dec(const Img2D &im, Work &w, uint32_t key)
+{
+    const int64_t y = key / uint32_t(im.cols), x = key - y * im.cols;
+    dec_u8(w.segcnt, im.seg_base + y * im.tiles_x + x / TW);
+}
+
+// Union of two nodes of one image; the root with the larger key is linked under the other.
+__device__ void gunion2d(const Img2D &im, Work &w, uint32_t a, uint32_t b)
+{
+    for (;;) {
+        a = gfind(w.gp, a);
+        b = gfind(w.gp, b);
+        if (a == b) return;
+        uint32_t ka = w.nkey[a], kb = w.nkey[b];
+        if (ka < kb) {
+            uint32_t t = a; a = b; b = t;
+            t = ka; ka = kb; kb = t;
+        }
+        if (atomicCAS(&w.gp[a], a, b) == a) {
+            link_dec(im, w, ka);
+            return;
+        }
+    }
+}
+
+}  // namespace
+
+constexpr int K2_NT = TBH + TBW;
+
+__global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
+{
+    __shared__ uint32_t qslot;
+    ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
+    for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
+        const Img2D im = L.get(t);
+        const int64_t lt = t - im.tile_base;
+        const int ty = int(lt / im.tiles_x), tx = int(lt - int64_t(ty) * im.tiles_x);
+        const int nbr = (min(TH, im.rows - ty * TH) + 1) >> 1;
+        const int nbc = (min(TW, im.cols - tx * TW) + 1) >> 1;
+        const int p = threadIdx.x;
+        const uint16_t *pe = w.perim;
+        if (p < TBH) {
+            // Right border: neighbours in the tile to the right, same tile row.
+            const int r = p;
+            if (r >= nbr || tx + 1 >= im.tiles_x) continue;
+            const uint32_t A = pe[t * NPERIM + 2 * TBW + TBH + r];
+            if (!A) continue;
+            const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
+            const int64_t t2 = t + 1;
+#pragma unroll
+            for (int d = -1; d <= 1; ++d) {
+                const int rr = r + d;
+                if (rr < 0 || rr >= nbr) continue;
+                const uint32_t B = pe[t2 * NPERIM + 2 * TBW + rr];
+                if (!B) continue;
+                const uint32_t mB = B & 15u;
+                const bool c = d == 0 ? ((mA & 0xAu) && (mB & 0x5u))
+                                      : d < 0 ? ((mA & 2u) && (mB & 4u)) : ((mA & 8u) && (mB & 1u));
+                if (c) gunion2d(im, w, nA, uint32_t(t2 * MAXB + (B >> 4)));
+            }
+        } else {
+            // Bottom border: neighbours in the tile row below (including the diagonal tiles).
+            const int c = p - TBH;
+            if (c >= nbc || ty + 1 >= im.tiles_y) continue;
+            const uint32_t A = pe[t * NPERIM + TBW + c];
+            if (!A) continue;
+            const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
+#pragma unroll
+            for (int d = -1; d <= 1; ++d) {
+                int cc = c + d;
+                int64_t t2 = t + im.tiles_x;
+                if (cc < 0) {
+                    if (tx == 0) continue;
+                    t2 -= 1;
+                    cc = TBW - 1;
+                } else if (cc >= nbc) {
+                    if (tx + 1 >= im.tiles_x) continue;
+                    t2 += 1;
+                    cc = 0;
+                }
+                const uint32_t B = pe[t2 * NPERIM + cc];
+                if (!B) continue;
+                const uint32_t mB = B & 15u;
+                const bool cn = d == 0 ? ((mA & 0xCu) && (mB & 0x3u))
+                                       : d < 0 ? ((mA & 4u) && (mB & 2u)) : ((mA & 8u) && (mB & 1u));
+                if (cn) gunion2d(im, w, nA, uint32_t(t2 * MAXB + (B >> 4)));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Post-merge ranks of the surviving border roots (one CTA per tile).
+// ---------------------------------------------------------------------------------------------
+__device__ void post_tile_2d(const ImgList2D &L, Work &w, int64_t t)
+{
+    __shared__ uint32_t LB[TH][TW / 32];   // first pixels of the tile's linked nodes
+    const Img2D im = L.get(t);
+    const int64_t lt = t - im.tile_base;
+    const int ty = int(lt / im.tiles_x), tx = int(lt - int64_t(ty) * im.tiles_x);
+    const int y0 = ty * TH, x0 = tx * TW;
+    const uint32_t nb = w.nb[t];
+    for (int i = threadIdx.x; i < TH * (TW / 32); i += blockDim.x) (&LB[0][0])[i] = 0;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        const int64_t node = t * MAXB + j;
+        if (w.gp[node] == uint32_t(node)) continue;
+        const uint32_t k = w.nkey[node];
+        const uint32_t y = k / uint32_t(im.cols);
+        const int ly = int(y) - y0, lx = int(k - y * uint32_t(im.cols)) - x0;
+        atomicOr(&LB[ly][lx >> 5], 1u << (lx & 31));
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        const int64_t node = t * MAXB + j;
+        if (w.gp[node] != uint32_t(node)) continue;
+        const uint32_t k = w.nkey[node];
+        const uint32_t y = k / uint32_t(im.cols);
+        const int ly = int(y) - y0, lx = int(k - y * uint32_t(im.cols)) - x0;
+        uint32_t cnt = __popc(LB[ly][lx >> 5] & ((1u << (lx & 31)) - 1u));
+        for (int q = 0; q < (lx >> 5); ++q) cnt += __popc(LB[ly][q]);
+        w.grank[node] = w.nlrank[node] - cnt;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Label resolve and write.
+// ---------------------------------------------------------------------------------------------
+constexpr int K3_NT = 256;
+
+__global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
+{
+    __shared__ __align__(16) uint16_t Ls[NBLK];
+    __shared__ uint32_t LT[NBLK];
+    __shared__ uint32_t RB[TH][TW / 32];
+    __shared__ uint32_t segb[TH];
+    __shared__ uint32_t qslot;
+
+    const int tid = threadIdx.x;
+    const uint16_t *lab = reinterpret_cast<const uint16_t *>(w.lab);
+    ItemLoop loop{w.queue ? w.queue + 4 : nullptr, w.n_tiles};
+    for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
+        const Img2D im = L.get(t);
+        const int64_t lt = t - im.tile_base;
+        const int ty = int(lt / im.tiles_x), tx = int(lt - int64_t(ty) * im.tiles_x);
+        const int y0 = ty * TH, x0 = tx * TW;
+        const int nrp = min(TH, im.rows - y0), ncp = min(TW, im.cols - x0);
+        const int nbr = (nrp + 1) >> 1, nbc = (ncp + 1) >> 1;
+        const uint32_t base0 = w.segpref[im.seg_base];
+
+        for (int i = tid; i < NBLK / 8; i += K3_NT)
+            reinterpret_cast<uint4 *>(Ls)[i] = reinterpret_cast<const uint4 *>(lab + t * NBLK)[i];
+        for (int i = tid; i < TH * (TW / 32); i += K3_NT) (&RB[0][0])[i] = 0;
+        if (tid < TH && tid < nrp)
+            segb[tid] = w.segpref[im.seg_base + int64_t(y0 + tid) * im.tiles_x + tx] - base0;
+        if (lt == 0 && tid == 0)
+            w.ncomp[im.index] = int64_t(w.segpref[im.seg_base + int64_t(im.rows) * im.tiles_x] - base0);
+        __syncthreads();
+
+        // Roots of this tile.
+        for (int b = tid; b < NBLK; b += K3_NT) {
+            const uint32_t e = Ls[b];
+            if (!(e >> 12) || (e & 0xFFFu) != uint32_t(b)) continue;
+            int dy, dx;
+            first_px(e >> 12, dy, dx);
+            const int y = 2 * (b / TBW) + dy, x = 2 * (b % TBW) + dx;
+            atomicOr(&RB[y][x >> 5], 1u << (x & 31));
+        }
+        __syncthreads();
+        const uint32_t nb = w.nb[t];
+        for (uint32_t j = tid; j < nb; j += K3_NT) {
+            const int64_t node = t * MAXB + j;
+            if (w.gp[node] == uint32_t(node)) continue;
+            const uint32_t rb = w.nroot[node];
+            int dy, dx;
+            first_px(Ls[rb] >> 12, dy, dx);
+            const int y = 2 * int(rb / TBW) + dy, x = 2 * int(rb % TBW) + dx;
+            atomicAnd(&RB[y][x >> 5], ~(1u << (x & 31)));
+        }
+        __syncthreads();
+        for (int b = tid; b < NBLK; b += K3_NT) {
+            const uint32_t e = Ls[b];
+            if (!(e >> 12) || (e & 0xFFFu) != uint32_t(b)) continue;
+            int dy, dx;
+            first_px(e >> 12, dy, dx);
+            const int y = 2 * (b / TBW) + dy, x = 2 * (b % TBW) + dx;
+            uint32_t rank = __popc(RB[y][x >> 5] & ((1u << (x & 31)) - 1u));
+            for (int k = 0; k < (x >> 5); ++k) rank += __popc(RB[y][k]);
+            LT[b] = 1u + segb[y] + rank;
+        }
+        __syncthreads();
+        for (uint32_t j = tid; j < nb; j += K3_NT) {
+            const int64_t node = t * MAXB + j;
+            if (w.gp[node] == uint32_t(node)) continue;
+            const uint32_t g = gfind_ro(w.gp, uint32_t(node));
+            const uint32_t kg = w.nkey[g];
+            const int64_t yg = kg / uint32_t(im.cols), xg = kg - yg * im.cols;
+            const uint32_t sb = w.segpref[im.seg_base + yg * im.tiles_x + xg / TW] - base0;
+            LT[w.nroot[node]] = 1u + sb + w.grank[g];
+        }
+        __syncthreads();
+
+        // Output: one int4 (4 pixels of one row) per unit.
+        const bool vec_ok = ((reinterpret_cast<uintptr_t>(im.out) | uintptr_t(im.out_pitch * 4)) & 15) == 0;
+        for (int u = tid; u < TH * (TW / 4); u += K3_NT) {
+            const int y = u / (TW / 4), q = u % (TW / 4);
+            if (y >= nrp || 4 * q >= ncp) continue;
+            const int br = y >> 1, h = (y & 1) * 2;
+            const uint32_t e0 = Ls[br * TBW + 2 * q];
+            const uint32_t e1 = 2 * q + 1 < nbc ? Ls[br * TBW + 2 * q + 1] : 0u;
+            const uint32_t m0 = e0 >> 12, m1 = e1 >> 12;
+            const uint32_t l0 = m0 ? LT[e0 & 0xFFFu] : 0u, l1 = m1 ? LT[e1 & 0xFFFu] : 0u;
+            int4 v;
+            v.x = ((m0 >> h) & 1u) ? int(l0) : 0;
+            v.y = ((m0 >> (h + 1)) & 1u) ? int(l0) : 0;
+            v.z = ((m1 >> h) & 1u) ? int(l1) : 0;
+            v.w = ((m1 >> (h + 1)) & 1u) ? int(l1) : 0;
+            int32_t *dst = im.out + int64_t(y0 + y) * im.out_pitch + x0 + 4 * q;
+            if (vec_ok && 4 * q + 4 <= ncp) {
+                __stcs(reinterpret_cast<int4 *>(dst), v);
+            } else {
+                const int n = min(4, ncp - 4 * q);
+                dst[0] = v.x;
+                if (n > 1) dst[1] = v.y;
+                if (n > 2) dst[2] = v.z;
+                if (n > 3) dst[3] = v.w;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Post-merge pass: border-root ranks (items < n_tiles) and scan-chunk sums (the rest).
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kPostThreads) k_post_2d(ImgList2D L, Work w)
+{
+    __shared__ uint32_t tmp[kPostThreads / 32 + 1];
+    __shared__ uint32_t qslot;
+    const int64_t n = w.n_tiles + w.n_chunks;
+    ItemLoop loop{w.queue ? w.queue + 2 : nullptr, n};
+    for (int64_t it = loop.first(&qslot); it < n; it = loop.next(it, &qslot)) {
+        if (it < w.n_tiles) post_tile_2d(L, w, it);
+        else chunk_sum<kPostThreads>(w, it - w.n_tiles, tmp);
+    }
+}
+
+}  // namespace be

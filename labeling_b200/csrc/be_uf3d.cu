@@ -1,0 +1,612 @@
+// be_uf3d.cu -- 3D Block-Equivalence labeling, union-find form (26-connectivity, 2x2x2 blocks).
+//
+// Replaces the reference's BLEQ3D_Init / BLEQ3D_Scan / BLEQ3D_Analyze / BLEQ3D_SetFinalLabels
+// (LabelingAlgs.cl:740-979) and their host loop (LabelingAlgs.cpp:1443-1536) with the same
+// five-launch structure as the 2D pipeline (be_uf2d.cu):
+//
+//   k_tile_local_3d   one CTA per 16 x 32 x 64-voxel tile (8 x 16 x 32 blocks): 16-byte loads,
+//                     8-bit block masks, shared-memory union-find over the 13 preceding
+//                     neighbours, flatten, per-component first-voxel key (atomicMin), one uint32
+//                     per block, segment root counts, border components exported as nodes.
+//   k_merge_3d        global union-find over nodes across the +d0 / +d1 / +d2 tile faces.
+//   k_post_3d         ranks of surviving border roots + scan-chunk sums.
+//   k_segscan         exclusive scan of the segment counts (be_scan.cu).
+//   k_tile_write_3d   resolves canonical labels and writes int32 voxels with 16-byte stores.
+//
+// Volume layout is the reference's cv::Mat 3-D order [d0][d1][d2] with d2 fastest
+// (Read3DImage, main.cpp:191-203; kernel addressing x*h*d + y*d + z, LabelingAlgs.cl:974).
+// Mask bit v = 4i + 2j + k is the voxel at offset (i, j, k) in (d0, d1, d2); the lowest set bit
+// is the block's first voxel in raster order.
+//
+// Block connectivity.  Two blocks A and B = A + d are 26-connected iff A has a foreground voxel
+// on its side facing B and B has one on its side facing A: along an axis with d = -1 only offset
+// 0 of A and offset 1 of B can touch, along an axis with d = 0 every offset can.  This is the
+// predicate the reference evaluates voxel by voxel with TEST_CONN1/2/4 (LabelingAlgs.cl:770-856).
+//
+// Within a tile the union keeps the smaller block index as the root; the component's key (its
+// smallest first-voxel index) is then gathered per root with atomicMin.
+#include "be_common.cuh"
+#include "be_kernels.h"
+#include "be_scan.cuh"
+
+namespace be {
+
+namespace {
+
+constexpr int TB0 = T3_TB0, TB1 = T3_TB1, TB2 = T3_TB2;   // tile in blocks
+constexpr int TX = 2 * TB0, TY = 2 * TB1, TZ = 2 * TB2;   // tile in voxels
+constexpr int NBLK = T3_NBLK;
+constexpr int NPERIM = T3_NPERIM;
+constexpr int MAXB = T3_MAXB;
+constexpr int NT = kT3Threads;
+constexpr int ZG = TB2 / 8;                 // 8-block groups along d2
+constexpr int ITEMS = TB0 * TB1 * ZG;       // items of 8 blocks
+constexpr int RBW = TZ / 32;                // root-bitmap words per voxel row
+constexpr uint32_t ROOT_FLAG = 1u << 23;
+
+static_assert(NBLK <= (1 << 13), "tile-local block index must fit the entry payload");
+static_assert(TX * TY * TZ <= (1 << 23), "tile-local key must fit the entry payload");
+static_assert(ITEMS % NT == 0, "items must divide evenly");
+static_assert(NPERIM < 65536 && MAXB < 4096, "border encodings");
+
+// Voxel-offset selector of a block side along one axis: offset 0 (d = -1), 1 (d = +1) or both.
+__device__ __forceinline__ uint32_t sel_axis(int axis, int d)
+{
+    // bit v = 4i + 2j + k; axis 0 -> i, 1 -> j, 2 -> k
+    constexpr uint32_t lo[3] = {0x0Fu, 0x33u, 0x55u};
+    constexpr uint32_t hi[3] = {0xF0u, 0xCCu, 0xAAu};
+    return d < 0 ? lo[axis] : d > 0 ? hi[axis] : 0xFFu;
+}
+
+__device__ __forceinline__ uint32_t side_sel(int dx, int dy, int dz)
+{
+    return sel_axis(0, dx) & sel_axis(1, dy) & sel_axis(2, dz);
+}
+
+__device__ __forceinline__ bool bconn(uint32_t ma, uint32_t mb, int dx, int dy, int dz)
+{
+    return (ma & side_sel(dx, dy, dz)) && (mb & side_sel(-dx, -dy, -dz));
+}
+
+__device__ __forceinline__ int blk(int b0, int b1, int b2) { return (b0 * TB1 + b1) * TB2 + b2; }
+
+// Tile-local key of the first voxel of a block.
+__device__ __forceinline__ uint32_t local_key(int b, uint32_t m)
+{
+    const int v = __ffs(m) - 1;
+    const int b2 = b % TB2, b1 = (b / TB2) % TB1, b0 = b / (TB1 * TB2);
+    const int X = 2 * b0 + (v >> 2), Y = 2 * b1 + ((v >> 1) & 1), Z = 2 * b2 + (v & 1);
+    return uint32_t((X * TY + Y) * TZ + Z);
+}
+
+__device__ __forceinline__ uint32_t nib2byte(uint32_t x)
+{
+    x &= 0xFFFFu;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    return x;
+}
+
+// 16 foreground bits along d2 (8 blocks x 2 voxels) -> per block 2-bit field in its byte.
+__device__ __forceinline__ uint2 pairs_to_bytes(uint32_t bits16)
+{
+    const uint32_t n = pairs_to_nibbles(bits16);
+    return make_uint2(nib2byte(n), nib2byte(n >> 16));
+}
+
+// Border faces: 0 = -d0, 1 = +d0, 2 = -d1, 3 = +d1, 4 = -d2, 5 = +d2.
+__device__ __forceinline__ int face_base(int f)
+{
+    constexpr int sz[6] = {TB1 * TB2, TB1 * TB2, TB0 * TB2, TB0 * TB2, TB0 * TB1, TB0 * TB1};
+    int b = 0;
+    for (int i = 0; i < f; ++i) b += sz[i];
+    return b;
+}
+
+// The four voxels of a block on face f, as bits (a*2 + b) over the two tangent axes in order.
+__device__ __forceinline__ uint32_t face_bits(uint32_t m, int f)
+{
+    const int axis = f >> 1, off = f & 1;
+    uint32_t r = 0;
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+        const int i = v >> 2, j = (v >> 1) & 1, k = v & 1;
+        const int o = axis == 0 ? i : axis == 1 ? j : k;
+        if (o != off || !((m >> v) & 1u)) continue;
+        const int ta = axis == 0 ? j : i, tb = axis == 2 ? j : k;
+        r |= 1u << (ta * 2 + tb);
+    }
+    return r;
+}
+
+// Selector over face bits (a*2 + b) for the tangent offsets (da, db).
+__device__ __forceinline__ uint32_t face_sel(int da, int db)
+{
+    const uint32_t sa = da < 0 ? 0x3u : da > 0 ? 0xCu : 0xFu;
+    const uint32_t sb = db < 0 ? 0x5u : db > 0 ? 0xAu : 0xFu;
+    return sa & sb;
+}
+
+struct TileGeo {
+    int tx0, tx1, tx2;      // tile coordinates
+    int x0, y0, z0;         // first voxel
+    int nx, ny, nz;         // valid voxels
+    int n0, n1, n2;         // valid blocks
+};
+
+__device__ __forceinline__ TileGeo tile_geo(const Img3D &im, int64_t t)
+{
+    TileGeo g;
+    const int64_t lt = t - im.tile_base;
+    g.tx2 = int(lt % im.t2);
+    g.tx1 = int((lt / im.t2) % im.t1);
+    g.tx0 = int(lt / (int64_t(im.t2) * im.t1));
+    g.x0 = g.tx0 * TX; g.y0 = g.tx1 * TY; g.z0 = g.tx2 * TZ;
+    g.nx = min(TX, im.d0 - g.x0); g.ny = min(TY, im.d1 - g.y0); g.nz = min(TZ, im.d2 - g.z0);
+    g.n0 = (g.nx + 1) >> 1; g.n1 = (g.ny + 1) >> 1; g.n2 = (g.nz + 1) >> 1;
+    return g;
+}
+
+// Block position of border position p (face f, index q), when valid for this tile.
+__device__ __forceinline__ bool perim_pos3(int p, const TileGeo &g, int &f, int &b0, int &b1, int &b2)
+{
+    f = 0;
+    int q = p;
+    while (f < 5 && q >= face_base(f + 1) - face_base(f)) { q -= face_base(f + 1) - face_base(f); ++f; }
+    const int axis = f >> 1, hi = f & 1;
+    if (axis == 0) { b0 = hi ? g.n0 - 1 : 0; b1 = q / TB2; b2 = q % TB2; }
+    else if (axis == 1) { b1 = hi ? g.n1 - 1 : 0; b0 = q / TB2; b2 = q % TB2; }
+    else { b2 = hi ? g.n2 - 1 : 0; b0 = q / TB1; b1 = q % TB1; }
+    return b0 < g.n0 && b1 < g.n1 && b2 < g.n2;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Tile-local labeling.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
+{
+    __shared__ uint32_t P[NBLK];
+    __shared__ uint32_t KM[NBLK];
+    __shared__ __align__(16) uint8_t M[NBLK];
+    __shared__ uint32_t RB[TX * TY * RBW];
+    __shared__ uint32_t BF[NBLK / 32];
+    __shared__ uint32_t BP[NBLK / 32];
+    __shared__ uint32_t tmp[NT / 32 + 1];
+    __shared__ uint32_t qslot;
+
+    const int tid = threadIdx.x;
+    uint32_t *lab = reinterpret_cast<uint32_t *>(w.lab);
+    ItemLoop loop{w.queue ? w.queue + 0 : nullptr, w.n_tiles};
+    for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
+        const Img3D im = L.get(t);
+        const TileGeo g = tile_geo(im, t);
+        const uint32_t thr4 = uint32_t(im.thr) * 0x01010101u;
+        const int64_t rs0 = int64_t(im.d1) * im.d2;   // stride of d0 in voxels
+
+        for (int i = tid; i < TX * TY * RBW; i += NT) RB[i] = 0;
+        for (int i = tid; i < NBLK; i += NT) KM[i] = kNone;
+        if (tid < NBLK / 32) BF[tid] = 0;
+
+        // Phase A: masks and runs along d2.
+        uint64_t masks[ITEMS / NT];
+#pragma unroll
+        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
+            const int it = tid + it_i * NT;
+            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
+            uint2 acc = make_uint2(0, 0);
+            if (b0 < g.n0 && b1 < g.n1 && 16 * zg < g.nz) {
+                const int zz = g.z0 + 16 * zg;
+                const int n = min(16, g.nz - 16 * zg);
+#pragma unroll
+                for (int ij = 0; ij < 4; ++ij) {
+                    const int i = ij >> 1, j = ij & 1;
+                    const int X = g.x0 + 2 * b0 + i, Y = g.y0 + 2 * b1 + j;
+                    if (X >= im.d0 || Y >= im.d1) continue;
+                    const uint8_t *row = im.in + X * rs0 + int64_t(Y) * im.d2 + zz;
+                    uint32_t bits = 0;
+                    if (n == 16 && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+                        bits = fg16(__ldg(reinterpret_cast<const uint4 *>(row)), thr4);
+                    } else {
+                        for (int z = 0; z < n; ++z) bits |= uint32_t(row[z] > im.thr) << z;
+                    }
+                    const uint2 pb = pairs_to_bytes(bits);
+                    const int sh = 4 * i + 2 * j;
+                    acc.x |= pb.x << sh;
+                    acc.y |= pb.y << sh;
+                }
+            }
+            masks[it_i] = (uint64_t(acc.y) << 32) | acc.x;
+            const int bb = blk(b0, b1, 8 * zg);
+            *reinterpret_cast<uint2 *>(&M[bb]) = acc;
+            uint32_t run = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t m = uint32_t(masks[it_i] >> (8 * k)) & 0xFFu;
+                if (!m) continue;
+                const uint32_t mp = k ? uint32_t(masks[it_i] >> (8 * (k - 1))) & 0xFFu : 0u;
+                if (!(k && bconn(m, mp, 0, 0, -1))) run = bb + k;
+                P[bb + k] = run;
+            }
+        }
+        __syncthreads();
+
+        // Phase B: merges with the 13 preceding neighbours inside the tile.
+#pragma unroll
+        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
+            const int it = tid + it_i * NT;
+            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
+            const uint64_t ms = masks[it_i];
+            if (!ms) continue;
+#pragma unroll 1
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
+                if (!m) continue;
+                const int b2 = 8 * zg + k;
+                const int b = blk(b0, b1, b2);
+                if (k == 0 && b2 > 0) {
+                    const uint32_t mz = M[b - 1];
+                    if (bconn(m, mz, 0, 0, -1)) smerge(P, b, b - 1);
+                }
+                for (int dx = -1; dx <= 0; ++dx) {
+                    if (b0 + dx < 0) continue;
+                    for (int dy = -1; dy <= 1; ++dy) {
+                        if (dx == 0 && dy >= 0) break;
+                        const int y1 = b1 + dy;
+                        if (y1 < 0 || y1 >= TB1) continue;
+                        for (int dz = -1; dz <= 1; ++dz) {
+                            const int z2 = b2 + dz;
+                            if (z2 < 0 || z2 >= TB2) continue;
+                            const int nbk = blk(b0 + dx, y1, z2);
+                            const uint32_t mn = M[nbk];
+                            if (mn && bconn(m, mn, dx, dy, dz)) smerge(P, b, nbk);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        // Phase C: flatten and per-component first-voxel key.
+#pragma unroll
+        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
+            const int it = tid + it_i * NT;
+            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
+            const uint64_t ms = masks[it_i];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
+                if (!m) continue;
+                const int b = blk(b0, b1, 8 * zg + k);
+                const uint32_t root = sfind(P, b);
+                P[b] = root;
+                atomicMin(&KM[root], local_key(b, m));
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
+            const int it = tid + it_i * NT;
+            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
+            const uint64_t ms = masks[it_i];
+            const int bb = blk(b0, b1, 8 * zg);
+            uint32_t e[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
+                e[k] = 0;
+                if (!m) continue;
+                const int b = bb + k;
+                const uint32_t root = P[b];
+                if (root == uint32_t(b)) {
+                    const uint32_t key = KM[b];
+                    e[k] = (m << 24) | ROOT_FLAG | key;
+                    const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
+                    atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
+                } else {
+                    e[k] = (m << 24) | root;
+                }
+            }
+            uint4 *dst = reinterpret_cast<uint4 *>(lab + t * NBLK + bb);
+            dst[0] = make_uint4(e[0], e[1], e[2], e[3]);
+            dst[1] = make_uint4(e[4], e[5], e[6], e[7]);
+        }
+        __syncthreads();
+
+        // Phase D: segment counts and border nodes.
+        for (int r = tid; r < TX * TY; r += NT) {
+            const int X = r / TY, Y = r % TY;
+            if (X >= g.nx || Y >= g.ny) continue;
+            uint32_t cnt = 0;
+#pragma unroll
+            for (int k = 0; k < RBW; ++k) cnt += __popc(RB[r * RBW + k]);
+            w.segcnt[im.seg_base + (int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.t2 + g.tx2] = uint8_t(cnt);
+        }
+        for (int p = tid; p < NPERIM; p += NT) {
+            int f, b0, b1, b2;
+            if (!perim_pos3(p, g, f, b0, b1, b2)) continue;
+            const int b = blk(b0, b1, b2);
+            if (!M[b]) continue;
+            const uint32_t rb = P[b];
+            atomicOr(&BF[rb >> 5], 1u << (rb & 31));
+        }
+        __syncthreads();
+        uint32_t nb;
+        const uint32_t pre = block_exscan<NT>(tid < NBLK / 32 ? __popc(BF[tid]) : 0u, tmp, &nb);
+        if (tid < NBLK / 32) BP[tid] = pre;
+        __syncthreads();
+        if (tid < NBLK / 32) {
+            uint32_t bits = BF[tid];
+            uint32_t j = pre;
+            while (bits) {
+                const int bit = __ffs(bits) - 1;
+                bits &= bits - 1;
+                const uint32_t rb = tid * 32 + bit;
+                const uint32_t key = KM[rb];
+                const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
+                const uint32_t *row = &RB[(X * TY + Y) * RBW];
+                uint32_t rank = __popc(row[Z >> 5] & ((1u << (Z & 31)) - 1u));
+                for (int k = 0; k < (Z >> 5); ++k) rank += __popc(row[k]);
+                const int64_t node = t * MAXB + j;
+                w.nroot[node] = uint16_t(rb);
+                w.nkey[node] = uint32_t((int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.d2 + (g.z0 + Z));
+                w.nlrank[node] = uint16_t(rank);
+                w.gp[node] = uint32_t(node);
+                ++j;
+            }
+        }
+        for (int p = tid; p < NPERIM; p += NT) {
+            int f, b0, b1, b2;
+            uint16_t ent = 0;
+            if (perim_pos3(p, g, f, b0, b1, b2)) {
+                const int b = blk(b0, b1, b2);
+                const uint32_t m = M[b];
+                if (m) {
+                    const uint32_t rb = P[b];
+                    const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
+                    ent = uint16_t((j << 4) | face_bits(m, f));
+                }
+            }
+            w.perim[t * NPERIM + p] = ent;
+        }
+        if (tid == 0) w.nb[t] = nb;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Cross-tile merge over the +d0, +d1 and +d2 faces.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+__device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
+{
+    for (;;) {
+        a = gfind(w.gp, a);
+        b = gfind(w.gp, b);
+        if (a == b) return;
+        uint32_t ka = w.nkey[a], kb = w.nkey[b];
+        if (ka < kb) {
+            uint32_t t = a; a = b; b = t;
+            t = ka; ka = kb; kb = t;
+        }
+        if (atomicCAS(&w.gp[a], a, b) == a) {
+            const int64_t row = ka / uint32_t(im.d2), z = ka - row * im.d2;
+            dec_u8(w.segcnt, im.seg_base + row * im.t2 + z / TZ);
+            return;
+        }
+    }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work w)
+{
+    __shared__ uint32_t qslot;
+    constexpr int NPLUS = TB1 * TB2 + TB0 * TB2 + TB0 * TB1;
+    ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
+    for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
+        const Img3D im = L.get(t);
+        const TileGeo g = tile_geo(im, t);
+        const int nbk[3] = {(im.d0 + 1) >> 1, (im.d1 + 1) >> 1, (im.d2 + 1) >> 1};
+        const int tb[3] = {TB0, TB1, TB2};
+        const int tc[3] = {g.tx0, g.tx1, g.tx2};
+        const int tn[3] = {im.t0, im.t1, im.t2};
+        for (int p = threadIdx.x; p < NPLUS; p += kT3MergeThreads) {
+            int axis, q;
+            if (p < TB1 * TB2) { axis = 0; q = p; }
+            else if (p < TB1 * TB2 + TB0 * TB2) { axis = 1; q = p - TB1 * TB2; }
+            else { axis = 2; q = p - TB1 * TB2 - TB0 * TB2; }
+            if (tc[axis] + 1 >= tn[axis]) continue;
+            const int f = 2 * axis + 1;
+            int lb[3];
+            if (axis == 0) { lb[0] = g.n0 - 1; lb[1] = q / TB2; lb[2] = q % TB2; }
+            else if (axis == 1) { lb[1] = g.n1 - 1; lb[0] = q / TB2; lb[2] = q % TB2; }
+            else { lb[2] = g.n2 - 1; lb[0] = q / TB1; lb[1] = q % TB1; }
+            if (lb[0] >= g.n0 || lb[1] >= g.n1 || lb[2] >= g.n2) continue;
+            const uint32_t A = w.perim[t * NPERIM + face_base(f) + q];
+            if (!A) continue;
+            const uint32_t fa = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
+            const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;   // tangent axes in order
+            for (int da = -1; da <= 1; ++da) {
+                for (int db = -1; db <= 1; ++db) {
+                    if (!(fa & face_sel(da, db))) continue;
+                    int gbk[3];
+                    gbk[axis] = tc[axis] * tb[axis] + lb[axis] + 1;
+                    gbk[ax1] = tc[ax1] * tb[ax1] + lb[ax1] + da;
+                    gbk[ax2] = tc[ax2] * tb[ax2] + lb[ax2] + db;
+                    if (gbk[ax1] < 0 || gbk[ax1] >= nbk[ax1] || gbk[ax2] < 0 || gbk[ax2] >= nbk[ax2]) continue;
+                    int tt[3], lc[3];
+                    for (int a = 0; a < 3; ++a) { tt[a] = gbk[a] / tb[a]; lc[a] = gbk[a] - tt[a] * tb[a]; }
+                    const int64_t t2i = im.tile_base + (int64_t(tt[0]) * im.t1 + tt[1]) * im.t2 + tt[2];
+                    const int qb = axis == 0 ? lc[1] * TB2 + lc[2] : axis == 1 ? lc[0] * TB2 + lc[2]
+                                                                              : lc[0] * TB1 + lc[1];
+                    const uint32_t B = w.perim[t2i * NPERIM + face_base(2 * axis) + qb];
+                    if (!B) continue;
+                    if (!((B & 15u) & face_sel(-da, -db))) continue;
+                    gunion3d(im, w, nA, uint32_t(t2i * MAXB + (B >> 4)));
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Post-merge ranks of surviving border roots, and scan-chunk sums.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+__device__ void post_tile_3d(const ImgList3D &L, Work &w, int64_t t)
+{
+    __shared__ uint32_t LB[TX * TY * RBW];   // keys of linked nodes
+    const Img3D im = L.get(t);
+    const TileGeo g = tile_geo(im, t);
+    const uint32_t nb = w.nb[t];
+    for (int i = threadIdx.x; i < TX * TY * RBW; i += blockDim.x) LB[i] = 0;
+    __syncthreads();
+    auto local = [&](uint32_t key, int &X, int &Y, int &Z) {
+        const uint32_t row = key / uint32_t(im.d2);
+        Z = int(key - row * uint32_t(im.d2)) - g.z0;
+        const uint32_t xg = row / uint32_t(im.d1);
+        Y = int(row - xg * uint32_t(im.d1)) - g.y0;
+        X = int(xg) - g.x0;
+    };
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        const int64_t node = t * MAXB + j;
+        if (w.gp[node] == uint32_t(node)) continue;
+        int X, Y, Z;
+        local(w.nkey[node], X, Y, Z);
+        atomicOr(&LB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        const int64_t node = t * MAXB + j;
+        if (w.gp[node] != uint32_t(node)) continue;
+        int X, Y, Z;
+        local(w.nkey[node], X, Y, Z);
+        const uint32_t *row = &LB[(X * TY + Y) * RBW];
+        uint32_t cnt = __popc(row[Z >> 5] & ((1u << (Z & 31)) - 1u));
+        for (int k = 0; k < (Z >> 5); ++k) cnt += __popc(row[k]);
+        w.grank[node] = w.nlrank[node] - cnt;
+    }
+    __syncthreads();
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kPostThreads) k_post_3d(ImgList3D L, Work w)
+{
+    __shared__ uint32_t tmp[kPostThreads / 32 + 1];
+    __shared__ uint32_t qslot;
+    const int64_t n = w.n_tiles + w.n_chunks;
+    ItemLoop loop{w.queue ? w.queue + 2 : nullptr, n};
+    for (int64_t it = loop.first(&qslot); it < n; it = loop.next(it, &qslot)) {
+        if (it < w.n_tiles) post_tile_3d(L, w, it);
+        else chunk_sum<kPostThreads>(w, it - w.n_tiles, tmp);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Label resolve and write.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
+{
+    __shared__ __align__(16) uint32_t Ls[NBLK];
+    __shared__ uint32_t LT[NBLK];
+    __shared__ uint32_t RB[TX * TY * RBW];
+    __shared__ uint32_t segb[TX * TY];
+    __shared__ uint32_t qslot;
+
+    const int tid = threadIdx.x;
+    const uint32_t *lab = reinterpret_cast<const uint32_t *>(w.lab);
+    ItemLoop loop{w.queue ? w.queue + 4 : nullptr, w.n_tiles};
+    for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
+        const Img3D im = L.get(t);
+        const TileGeo g = tile_geo(im, t);
+        const uint32_t base0 = w.segpref[im.seg_base];
+        const int64_t rs0 = int64_t(im.d1) * im.d2;
+
+        for (int i = tid; i < NBLK / 4; i += NT)
+            reinterpret_cast<uint4 *>(Ls)[i] = reinterpret_cast<const uint4 *>(lab + t * NBLK)[i];
+        for (int i = tid; i < TX * TY * RBW; i += NT) RB[i] = 0;
+        for (int r = tid; r < TX * TY; r += NT) {
+            const int X = r / TY, Y = r % TY;
+            if (X < g.nx && Y < g.ny)
+                segb[r] = w.segpref[im.seg_base + (int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.t2 + g.tx2] - base0;
+        }
+        if (t == im.tile_base && tid == 0)
+            w.ncomp[im.index] = int64_t(w.segpref[im.seg_base + int64_t(im.d0) * im.d1 * im.t2] - base0);
+        __syncthreads();
+
+        for (int b = tid; b < NBLK; b += NT) {
+            const uint32_t e = Ls[b];
+            if (!(e & ROOT_FLAG)) continue;
+            const uint32_t key = e & (ROOT_FLAG - 1);
+            const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
+            atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
+        }
+        __syncthreads();
+        const uint32_t nb = w.nb[t];
+        for (uint32_t j = tid; j < nb; j += NT) {
+            const int64_t node = t * MAXB + j;
+            if (w.gp[node] == uint32_t(node)) continue;
+            const uint32_t key = Ls[w.nroot[node]] & (ROOT_FLAG - 1);
+            const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
+            atomicAnd(&RB[(X * TY + Y) * RBW + (Z >> 5)], ~(1u << (Z & 31)));
+        }
+        __syncthreads();
+        for (int b = tid; b < NBLK; b += NT) {
+            const uint32_t e = Ls[b];
+            if (!(e & ROOT_FLAG)) continue;
+            const uint32_t key = e & (ROOT_FLAG - 1);
+            const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
+            const uint32_t *row = &RB[(X * TY + Y) * RBW];
+            uint32_t rank = __popc(row[Z >> 5] & ((1u << (Z & 31)) - 1u));
+            for (int k = 0; k < (Z >> 5); ++k) rank += __popc(row[k]);
+            LT[b] = 1u + segb[X * TY + Y] + rank;
+        }
+        __syncthreads();
+        for (uint32_t j = tid; j < nb; j += NT) {
+            const int64_t node = t * MAXB + j;
+            if (w.gp[node] == uint32_t(node)) continue;
+            const uint32_t gn = gfind_ro(w.gp, uint32_t(node));
+            const uint32_t kg = w.nkey[gn];
+            const int64_t row = kg / uint32_t(im.d2), z = kg - row * im.d2;
+            const uint32_t sb = w.segpref[im.seg_base + row * im.t2 + z / TZ] - base0;
+            LT[w.nroot[node]] = 1u + sb + w.grank[gn];
+        }
+        __syncthreads();
+
+        // Output: units of 4 voxels along d2 (2 blocks).
+        for (int u = tid; u < TX * TY * (TZ / 4); u += NT) {
+            const int q = u % (TZ / 4), r = u / (TZ / 4);
+            const int X = r / TY, Y = r % TY;
+            if (X >= g.nx || Y >= g.ny || 4 * q >= g.nz) continue;
+            const int bb = blk(X >> 1, Y >> 1, 2 * q);
+            const uint32_t e0 = Ls[bb], e1 = (2 * q + 1 < TB2) ? Ls[bb + 1] : 0u;
+            const uint32_t m0 = e0 >> 24, m1 = e1 >> 24;
+            const uint32_t l0 = m0 ? ((e0 & ROOT_FLAG) ? LT[bb] : LT[e0 & 0x7FFFFFu]) : 0u;
+            const uint32_t l1 = m1 ? ((e1 & ROOT_FLAG) ? LT[bb + 1] : LT[e1 & 0x7FFFFFu]) : 0u;
+            const int sh = 4 * (X & 1) + 2 * (Y & 1);
+            int4 v;
+            v.x = ((m0 >> sh) & 1u) ? int(l0) : 0;
+            v.y = ((m0 >> (sh + 1)) & 1u) ? int(l0) : 0;
+            v.z = ((m1 >> sh) & 1u) ? int(l1) : 0;
+            v.w = ((m1 >> (sh + 1)) & 1u) ? int(l1) : 0;
+            int32_t *dst = im.out + (g.x0 + X) * rs0 + int64_t(g.y0 + Y) * im.d2 + g.z0 + 4 * q;
+            if (4 * q + 4 <= g.nz && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+                __stcs(reinterpret_cast<int4 *>(dst), v);
+            } else {
+                const int n = min(4, g.nz - 4 * q);
+                dst[0] = v.x;
+                if (n > 1) dst[1] = v.y;
+                if (n > 2) dst[2] = v.z;
+                if (n > 3) dst[3] = v.w;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace be

@@ -1,0 +1,107 @@
+"""2D parity on the GPU: every label map must equal the oracle's canonical labels bit for bit
+(integer work: the tolerance is exact) and the component count must match."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+ALGOS = [1, 2]   # BE_ALGO_UF, BE_ALGO_ITER
+
+
+def run2d(ctx, img, thr=0, algo=1, pitch_pad=0, offset=0):
+    import torch
+    import labeling_b200 as be
+    h, w = img.shape
+    buf = torch.zeros(h * (w + pitch_pad) + offset + 64, dtype=torch.uint8, device="cuda")
+    view = buf[offset:offset + h * (w + pitch_pad)].view(h, w + pitch_pad)[:, :w]
+    view.copy_(torch.from_numpy(img).cuda())
+    out = torch.full((h, w + pitch_pad), -7, dtype=torch.int32, device="cuda")[:, :w]
+    n = be.label2d(ctx, view, out, threshold=thr, algo=algo)
+    torch.cuda.synchronize()
+    return out.cpu().numpy(), n
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_golden_cases(ctx, golden, algo):
+    for (dim, name), c in golden.items():
+        if dim != "2d":
+            continue
+        lab, n = run2d(ctx, c["img"], int(c["thr"]), algo)
+        assert np.array_equal(lab, c["canon"]), (name, algo)
+        assert n == int(c["k"]), (name, algo)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_shapes_uf_vs_oracle(ctx, seed):
+    rng = np.random.default_rng(1000 + seed)
+    h = int(rng.choice([1, 2, 3, 63, 64, 65, 127, 129, 200, 511, 700]))
+    w = int(rng.choice([1, 2, 5, 255, 256, 257, 300, 513, 1000, 1023]))
+    p = float(rng.uniform(0.05, 0.95))
+    img = ((rng.random((h, w)) < p) * 255).astype(np.uint8)
+    ref, k = O.ccl2d(img)
+    lab, n = run2d(ctx, img, 0, 1)
+    assert np.array_equal(lab, ref) and n == k
+
+
+@pytest.mark.parametrize("p", [0.1, 0.4, 0.5, 0.6, 0.9])
+def test_2048_bernoulli_both_forms(ctx, p):
+    from labeling_b200 import workloads as W
+    img = W.bernoulli((2048, 2048), p, seed=int(p * 100))
+    ref, k = O.ccl2d(img)
+    for algo in ALGOS:
+        lab, n = run2d(ctx, img, 0, algo)
+        assert n == k and np.array_equal(lab, ref), algo
+
+
+@pytest.mark.parametrize("family", ["serpentine", "spiral", "disks"])
+def test_worst_case_paths(ctx, family):
+    from labeling_b200 import workloads as W
+    img = W.family_8192(family, seed=3, side=1536)
+    ref, k = O.ccl2d(img)
+    for algo in ALGOS:
+        lab, n = run2d(ctx, img, 0, algo)
+        assert n == k and np.array_equal(lab, ref), algo
+
+
+def test_pitch_offset_threshold(ctx):
+    rng = np.random.default_rng(7)
+    img = rng.integers(0, 256, (333, 517)).astype(np.uint8)
+    for thr in (0, 8, 128, 254):
+        ref, k = O.ccl2d(img, thr)
+        for pad, off in ((0, 0), (11, 3), (64, 16)):
+            lab, n = run2d(ctx, img, thr, 1, pad, off)
+            assert n == k and np.array_equal(lab, ref), (thr, pad, off)
+
+
+def test_edge_shapes(ctx):
+    for img in (np.zeros((1, 1), np.uint8), np.full((1, 1), 255, np.uint8),
+                np.full((1, 4097), 255, np.uint8), np.full((4097, 1), 255, np.uint8),
+                np.zeros((300, 300), np.uint8), np.full((300, 301), 255, np.uint8),
+                (np.indices((256, 256)).sum(0) % 2 * 255).astype(np.uint8)):
+        ref, k = O.ccl2d(img)
+        for algo in ALGOS:
+            lab, n = run2d(ctx, img, 0, algo)
+            assert n == k and np.array_equal(lab, ref), (img.shape, algo)
+
+
+def test_repeat_is_deterministic(ctx):
+    from labeling_b200 import workloads as W
+    img = W.bernoulli((1111, 2222), 0.45, seed=9)
+    a, na = run2d(ctx, img)
+    b, nb = run2d(ctx, img)
+    assert na == nb and np.array_equal(a, b)
+
+
+def test_host_api_and_reference_interface(ctx):
+    import labeling_b200 as be
+    from labeling_b200 import workloads as W
+    img = W.bernoulli((777, 555), 0.5, seed=11)
+    ref, k = O.ccl2d(img)
+    lab, n, us = be.label2d_host(ctx, img)
+    assert n == k and np.array_equal(lab, ref) and us > 0
+    lab2, us2 = be.make_labeler("bleq", gpu=True).Label(img)
+    assert np.array_equal(lab2, ref) and us2 > 0
+    with pytest.raises(be.BEError):
+        be.label2d_host(ctx, img, coh=be.COH_4)
