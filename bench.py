@@ -228,6 +228,10 @@ def bench_ours(args, rank, world, local_rank):
             torch.cuda.synchronize()
         ctx.set_stage_timing(False)
         step_ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
+    per_image = {}
+    for s_, ms_ in enumerate(step_ms):
+        per_image.setdefault(inputs[s_ % len(inputs)][0], []).append(ms_)
+    per_image = {k: round(float(np.mean(v)), 4) for k, v in per_image.items()}
     t_ms = float(sum(step_ms))
     if world > 1:
         tt = torch.tensor([t_ms], device=dev)
@@ -298,6 +302,7 @@ def bench_ours(args, rank, world, local_rank):
         "e2e": e2e, "roofline": roofline, "roofline_kernels": kernels,
         "gpu_launches": 5 * steps, "clocks": clocks,
         "components": {n: c for (n, _), c in zip(inputs, counts)},
+        "per_image_ms": per_image,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         budget = 20.0

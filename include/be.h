@@ -94,6 +94,12 @@ int be_label3d_host(be_ctx *ctx, const uint8_t *in, int32_t d0, int32_t d1, int3
                     int threshold, int algo, int32_t *out, int64_t *n_components,
                     double *elapsed_us);
 
+/* Report of the bounds-checked debug build (-DBE_BOUNDS_CHECK; no counterpart in the
+ * reference): out3 = {site, value low, value high} of the first failed index check of the last
+ * 2D (dims = 2) or 3D (dims = 3) union-find call, all zero when none failed.  Normal builds
+ * perform no checks and always report zeros. */
+int be_check_status(be_ctx *ctx, int dims, uint32_t *out3);
+
 /* Per-launch timing of plain calls (no counterpart in the reference, whose stopwatch covers the
  * whole DoOCLLabel call, LabelingTools.cpp:118-125).  When enabled, be_label2d / be_label3d
  * record a CUDA event before and after each of their launches; be_stage_times then returns the

@@ -22,7 +22,9 @@ from typing import Optional, Tuple
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libbe_b200.so")
+# BE_B200_LIB selects another build of the same ABI (e.g. the bounds-checked
+# libbe_b200_check.so made by `python -m labeling_b200.build --checked`).
+LIB_PATH = os.environ.get("BE_B200_LIB") or os.path.join(_HERE, "libbe_b200.so")
 
 BE_OK = 0
 STATUS = {0: "BE_OK", 1: "BE_ERR_INVALID", 2: "BE_ERR_OOM", 3: "BE_ERR_NO_CONVERGENCE",
@@ -60,6 +62,7 @@ def lib() -> ctypes.CDLL:
     l.be_label2d_host.argtypes = [vp, vp, i64, i32, i32, c_int, c_int, c_int, vp, i64, p64, pdbl]
     l.be_label3d_host.argtypes = [vp, vp, i32, i32, i32, c_int, c_int, vp, p64, pdbl]
     l.be_set_stage_timing.argtypes = [vp, c_int]
+    l.be_check_status.argtypes = [vp, c_int, ctypes.POINTER(ctypes.c_uint32)]
     l.be_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), c_int, ctypes.POINTER(c_int)]
     _lib = l
     return l
@@ -88,6 +91,12 @@ class Context:
     def check(self, rc: int) -> None:
         if rc:
             raise BEError(rc, lib().be_last_error(self._h).decode())
+
+    def check_status(self, dims: int):
+        """(site, value) of the first failed index check of the last call (checked builds)."""
+        out = (ctypes.c_uint32 * 3)()
+        self.check(lib().be_check_status(self.handle, dims, out))
+        return int(out[0]), int(out[1]) | (int(out[2]) << 32)
 
     def set_stage_timing(self, on: bool) -> None:
         self.check(lib().be_set_stage_timing(self.handle, int(on)))

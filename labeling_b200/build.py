@@ -20,6 +20,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libbe_b200.so")
+LIB_CHECK = os.path.join(PKG, "libbe_b200_check.so")   # bounds-checked debug build
 CLI = os.path.join(PKG, "labeling")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -55,8 +56,13 @@ def _stale(out: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose: bool = False, ptxas_info: bool = False, checked: bool = False) -> str:
+    """Builds libbe_b200.so, or with checked=True the bounds-checked libbe_b200_check.so
+    (-DBE_BOUNDS_CHECK: failed index checks are recorded and skipped, see be_check_status)."""
+    build_dir = BUILD + ("_check" if checked else "")
+    lib_path = LIB_CHECK if checked else LIB
+    flags = NVCC_FLAGS + (["-DBE_BOUNDS_CHECK"] if checked else [])
+    os.makedirs(build_dir, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh", ".hpp"))]
     headers.append(os.path.join(ROOT, "include", "be.h"))
     objs = []
@@ -65,16 +71,18 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         s = os.path.join(CSRC, src)
         if not os.path.exists(s):
             continue
-        o = os.path.join(BUILD, src + ".o")
+        o = os.path.join(build_dir, src + ".o")
         objs.append(o)
         if _stale(o, [s] + headers) or ptxas_info:
             extra = ["-Xptxas", "-v"] if ptxas_info else []
-            jobs.append([nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", s, "-o", o])
+            jobs.append([nvcc(), *ARCH, *flags, *extra, "-c", s, "-o", o])
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         for r in ex.map(lambda c: _run(c, verbose or ptxas_info), jobs):
             pass
-    if jobs or _stale(LIB, objs):
-        _run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-fPIC"], verbose)
+    if jobs or _stale(lib_path, objs):
+        _run([nvcc(), *ARCH, "-shared", "-o", lib_path, *objs, "-Xcompiler", "-fPIC"], verbose)
+    if checked:
+        return lib_path
     cli_srcs = [os.path.join(CSRC, s) for s in CLI_SOURCES if os.path.exists(os.path.join(CSRC, s))]
     if len(cli_srcs) == len(CLI_SOURCES) and _stale(CLI, cli_srcs + headers + [LIB]):
         _run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC,
@@ -87,6 +95,7 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas-info", action="store_true", help="print registers/spills per kernel")
+    ap.add_argument("--checked", action="store_true", help="build the bounds-checked debug library")
     a = ap.parse_args()
-    print(build(a.verbose, a.ptxas_info))
+    print(build(a.verbose, a.ptxas_info, a.checked))
     sys.exit(0)

@@ -286,6 +286,17 @@ int be_destroy(be_ctx *c)
 
 const char *be_last_error(const be_ctx *c) { return c ? c->err.c_str() : "no context"; }
 
+int be_check_status(be_ctx *c, int dims, uint32_t *out3)
+{
+    if (!c || !out3 || (dims != 2 && dims != 3)) return BE_ERR_INVALID;
+    out3[0] = out3[1] = out3[2] = 0;
+    const Work &w = dims == 2 ? c->ws2d.w : c->ws3d.w;
+    if (!w.err) return BE_OK;
+    cudaError_t e = cudaMemcpy(out3, w.err, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(c, e, "be_check_status");
+    return BE_OK;
+}
+
 int be_set_stage_timing(be_ctx *c, int enable)
 {
     if (!c) return BE_ERR_INVALID;
@@ -341,6 +352,9 @@ int be_label2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
         rc = c->ws2d.ensure(c, geometry_2d(), n_tiles, n_segs, 1);
         if (rc) return rc;
         ImgList2D L{nullptr, 1, im};
+#ifdef BE_BOUNDS_CHECK
+        cudaMemsetAsync(c->ws2d.w.err, 0, 16 * sizeof(uint32_t), s);
+#endif
         e = launch_uf2d(L, c->ws2d.w, c->sms, false, s, c->timing ? c->stage_ev : nullptr);
         c->timed_stages = c->timing ? kStages : 0;
         if (e != cudaSuccess) return cuda_error(c, e, "be_label2d launch");
@@ -384,6 +398,9 @@ int be_label3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
         rc = c->ws3d.ensure(c, geometry_3d(), n_tiles, n_segs, 1);
         if (rc) return rc;
         ImgList3D L{nullptr, 1, im};
+#ifdef BE_BOUNDS_CHECK
+        cudaMemsetAsync(c->ws3d.w.err, 0, 16 * sizeof(uint32_t), s);
+#endif
         e = launch_uf3d(L, c->ws3d.w, c->sms, false, s, c->timing ? c->stage_ev : nullptr);
         c->timed_stages = c->timing ? kStages : 0;
         if (e != cudaSuccess) return cuda_error(c, e, "be_label3d launch");

@@ -82,6 +82,25 @@ struct Work {
 constexpr int kScanChunk = 16384;   // segments per scan chunk (one CTA)
 
 // ---------------------------------------------------------------------------------------------
+// Bounds-checked build (-DBE_BOUNDS_CHECK): GUARD(w, cond, site, value) is false when `cond`
+// fails; the first failure of a launch records (site, value) in w.err[0..2] and the guarded
+// access is skipped.  In normal builds GUARD is the constant true and costs nothing.
+// ---------------------------------------------------------------------------------------------
+#ifdef BE_BOUNDS_CHECK
+__device__ __forceinline__ bool be_guard(uint32_t *err, bool ok, uint32_t site, uint64_t val)
+{
+    if (!ok && atomicCAS(err, 0u, site) == 0u) {
+        err[1] = uint32_t(val);
+        err[2] = uint32_t(val >> 32);
+    }
+    return ok;
+}
+#define GUARD(w, cond, site, val) be_guard((w).err, bool(cond), (site), uint64_t(val))
+#else
+#define GUARD(w, cond, site, val) (true)
+#endif
+
+// ---------------------------------------------------------------------------------------------
 // Small helpers.
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p)
@@ -112,8 +131,27 @@ __device__ __forceinline__ uint32_t pairs_to_nibbles(uint32_t x)
     return x;
 }
 
-// Union-find find over a shared-memory parent array (parents never exceed their child).
-__device__ __forceinline__ uint32_t sfind(const uint32_t *P, uint32_t a)
+// Union-find find over a shared-memory parent array (parents never exceed their child), with
+// path halving: each visited entry is pointed at its grandparent.  Every stored value is an
+// ancestor of the entry at the time it was read, so concurrent merges stay correct: a pointer
+// never leaves the entry's component, and a merge that loses a race to such a store retries
+// from the parent it displaced (see smerge).
+__device__ __forceinline__ uint32_t sfind(uint32_t *P, uint32_t a)
+{
+    uint32_t p = P[a];
+    while (p != a) {
+        const uint32_t g = P[p];
+        if (g != p) P[a] = g;
+        a = p;
+        p = g;
+    }
+    return a;
+}
+
+// Find without writes, for the flatten pass after all merges: no link can happen any more, so the
+// entry reached is the true root.  (Path halving is not allowed there: a halving store that lands
+// after the entry's owner wrote its root would point the entry back at an inner node.)
+__device__ __forceinline__ uint32_t sfind_ro(const uint32_t *P, uint32_t a)
 {
     uint32_t p = P[a];
     while (p != a) {

@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(K1_NT) k_tile_local_2d(ImgList2D L, Work w)
                 if (!m) continue;
                 const int c = 8 * g + k;
                 const uint32_t s = slot_of(r, c, m);
-                const uint32_t root = sfind(P, s);
+                const uint32_t root = sfind_ro(P, s);
                 P[s] = root;
                 const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
                 e[k] = (m << 12) | rb;
@@ -340,6 +340,7 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
             if (!A) continue;
             const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
             const int64_t t2 = t + 1;
+            uint32_t last = kNone;
 #pragma unroll
             for (int d = -1; d <= 1; ++d) {
                 const int rr = r + d;
@@ -349,7 +350,9 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
                 const uint32_t mB = B & 15u;
                 const bool c = d == 0 ? ((mA & 0xAu) && (mB & 0x5u))
                                       : d < 0 ? ((mA & 2u) && (mB & 4u)) : ((mA & 8u) && (mB & 1u));
-                if (c) gunion2d(im, w, nA, uint32_t(t2 * MAXB + (B >> 4)));
+                const uint32_t nB = uint32_t(t2 * MAXB + (B >> 4));
+                if (c && nB != last) gunion2d(im, w, nA, nB);
+                if (c) last = nB;
             }
         } else {
             // Bottom border: neighbours in the tile row below (including the diagonal tiles).
@@ -358,6 +361,7 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
             const uint32_t A = pe[t * NPERIM + TBW + c];
             if (!A) continue;
             const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
+            uint32_t last = kNone;
 #pragma unroll
             for (int d = -1; d <= 1; ++d) {
                 int cc = c + d;
@@ -376,7 +380,9 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
                 const uint32_t mB = B & 15u;
                 const bool cn = d == 0 ? ((mA & 0xCu) && (mB & 0x3u))
                                        : d < 0 ? ((mA & 4u) && (mB & 2u)) : ((mA & 8u) && (mB & 1u));
-                if (cn) gunion2d(im, w, nA, uint32_t(t2 * MAXB + (B >> 4)));
+                const uint32_t nB = uint32_t(t2 * MAXB + (B >> 4));
+                if (cn && nB != last) gunion2d(im, w, nA, nB);
+                if (cn) last = nB;
             }
         }
     }

@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
                 const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
                 if (!m) continue;
                 const int b = blk(b0, b1, 8 * zg + k);
-                const uint32_t root = sfind(P, b);
+                const uint32_t root = sfind_ro(P, b);
                 P[b] = root;
                 atomicMin(&KM[root], local_key(b, m));
             }
@@ -303,7 +303,8 @@ __global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
                     const uint32_t key = KM[b];
                     e[k] = (m << 24) | ROOT_FLAG | key;
                     const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
-                    atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
+                    if (GUARD(w, key < uint32_t(TX * TY * TZ), 101, key))
+                        atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
                 } else {
                     e[k] = (m << 24) | root;
                 }
@@ -321,7 +322,8 @@ __global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
             uint32_t cnt = 0;
 #pragma unroll
             for (int k = 0; k < RBW; ++k) cnt += __popc(RB[r * RBW + k]);
-            w.segcnt[im.seg_base + (int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.t2 + g.tx2] = uint8_t(cnt);
+            const int64_t si = im.seg_base + (int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.t2 + g.tx2;
+            if (GUARD(w, si >= 0 && si < w.n_segs, 104, si)) w.segcnt[si] = uint8_t(cnt);
         }
         for (int p = tid; p < NPERIM; p += NT) {
             int f, b0, b1, b2;
@@ -344,6 +346,8 @@ __global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
                 bits &= bits - 1;
                 const uint32_t rb = tid * 32 + bit;
                 const uint32_t key = KM[rb];
+                if (!GUARD(w, key < uint32_t(TX * TY * TZ) && j < uint32_t(MAXB), 102, (uint64_t(j) << 32) | key))
+                    break;
                 const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
                 const uint32_t *row = &RB[(X * TY + Y) * RBW];
                 uint32_t rank = __popc(row[Z >> 5] & ((1u << (Z & 31)) - 1u));
@@ -428,7 +432,10 @@ __global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work 
             const uint32_t A = w.perim[t * NPERIM + face_base(f) + q];
             if (!A) continue;
             const uint32_t fa = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
+            if (!GUARD(w, (A >> 4) < w.nb[t], 204, (uint64_t(t) << 16) | (A >> 4))) continue;
             const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;   // tangent axes in order
+            uint32_t done[9];
+            int ndone = 0;
             for (int da = -1; da <= 1; ++da) {
                 for (int db = -1; db <= 1; ++db) {
                     if (!(fa & face_sel(da, db))) continue;
@@ -442,10 +449,17 @@ __global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work 
                     const int64_t t2i = im.tile_base + (int64_t(tt[0]) * im.t1 + tt[1]) * im.t2 + tt[2];
                     const int qb = axis == 0 ? lc[1] * TB2 + lc[2] : axis == 1 ? lc[0] * TB2 + lc[2]
                                                                               : lc[0] * TB1 + lc[1];
+                    if (!GUARD(w, t2i >= 0 && t2i < w.n_tiles && qb >= 0 && qb < NPERIM, 201, t2i)) continue;
                     const uint32_t B = w.perim[t2i * NPERIM + face_base(2 * axis) + qb];
                     if (!B) continue;
                     if (!((B & 15u) & face_sel(-da, -db))) continue;
-                    gunion3d(im, w, nA, uint32_t(t2i * MAXB + (B >> 4)));
+                    const uint32_t nB = uint32_t(t2i * MAXB + (B >> 4));
+                    if (!GUARD(w, (B >> 4) < w.nb[t2i], 203, (uint64_t(t2i) << 16) | (B >> 4))) continue;
+                    bool seen = false;
+                    for (int q2 = 0; q2 < ndone; ++q2) seen |= done[q2] == nB;
+                    if (seen) continue;
+                    done[ndone++] = nB;
+                    gunion3d(im, w, nA, nB);
                 }
             }
         }
@@ -477,7 +491,8 @@ __device__ void post_tile_3d(const ImgList3D &L, Work &w, int64_t t)
         if (w.gp[node] == uint32_t(node)) continue;
         int X, Y, Z;
         local(w.nkey[node], X, Y, Z);
-        atomicOr(&LB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
+        if (GUARD(w, X >= 0 && X < TX && Y >= 0 && Y < TY && Z >= 0 && Z < TZ, 301, w.nkey[node]))
+            atomicOr(&LB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
     }
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
@@ -485,6 +500,7 @@ __device__ void post_tile_3d(const ImgList3D &L, Work &w, int64_t t)
         if (w.gp[node] != uint32_t(node)) continue;
         int X, Y, Z;
         local(w.nkey[node], X, Y, Z);
+        if (!GUARD(w, X >= 0 && X < TX && Y >= 0 && Y < TY && Z >= 0 && Z < TZ, 302, w.nkey[node])) continue;
         const uint32_t *row = &LB[(X * TY + Y) * RBW];
         uint32_t cnt = __popc(row[Z >> 5] & ((1u << (Z & 31)) - 1u));
         for (int k = 0; k < (Z >> 5); ++k) cnt += __popc(row[k]);
@@ -544,13 +560,15 @@ __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
             if (!(e & ROOT_FLAG)) continue;
             const uint32_t key = e & (ROOT_FLAG - 1);
             const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
-            atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
+            if (GUARD(w, key < uint32_t(TX * TY * TZ), 401, key))
+                atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
         }
         __syncthreads();
         const uint32_t nb = w.nb[t];
         for (uint32_t j = tid; j < nb; j += NT) {
             const int64_t node = t * MAXB + j;
             if (w.gp[node] == uint32_t(node)) continue;
+            if (!GUARD(w, w.nroot[node] < NBLK && (Ls[w.nroot[node] % NBLK] & ROOT_FLAG), 402, node)) continue;
             const uint32_t key = Ls[w.nroot[node]] & (ROOT_FLAG - 1);
             const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
             atomicAnd(&RB[(X * TY + Y) * RBW + (Z >> 5)], ~(1u << (Z & 31)));
@@ -573,7 +591,9 @@ __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
             const uint32_t gn = gfind_ro(w.gp, uint32_t(node));
             const uint32_t kg = w.nkey[gn];
             const int64_t row = kg / uint32_t(im.d2), z = kg - row * im.d2;
-            const uint32_t sb = w.segpref[im.seg_base + row * im.t2 + z / TZ] - base0;
+            const int64_t si = im.seg_base + row * im.t2 + z / TZ;
+            if (!GUARD(w, si >= 0 && si <= w.n_segs, 404, si)) continue;
+            const uint32_t sb = w.segpref[si] - base0;
             LT[w.nroot[node]] = 1u + sb + w.grank[gn];
         }
         __syncthreads();
@@ -586,6 +606,7 @@ __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
             const int bb = blk(X >> 1, Y >> 1, 2 * q);
             const uint32_t e0 = Ls[bb], e1 = (2 * q + 1 < TB2) ? Ls[bb + 1] : 0u;
             const uint32_t m0 = e0 >> 24, m1 = e1 >> 24;
+            if (!GUARD(w, !m0 || (e0 & ROOT_FLAG) || (Ls[(e0 & 0x7FFFFFu) % NBLK] & ROOT_FLAG && (e0 & 0x7FFFFFu) < NBLK), 403, e0)) continue;
             const uint32_t l0 = m0 ? ((e0 & ROOT_FLAG) ? LT[bb] : LT[e0 & 0x7FFFFFu]) : 0u;
             const uint32_t l1 = m1 ? ((e1 & ROOT_FLAG) ? LT[bb + 1] : LT[e1 & 0x7FFFFFu]) : 0u;
             const int sh = 4 * (X & 1) + 2 * (Y & 1);

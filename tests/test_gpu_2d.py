@@ -105,3 +105,14 @@ def test_host_api_and_reference_interface(ctx):
     assert np.array_equal(lab2, ref) and us2 > 0
     with pytest.raises(be.BEError):
         be.label2d_host(ctx, img, coh=be.COH_4)
+
+
+@pytest.mark.parametrize("p", [0.41, 0.45, 0.6])
+def test_large_image_repeated(ctx, p):
+    """4096^2 near the 8-connectivity percolation threshold, three runs, each exact."""
+    from labeling_b200 import workloads as W
+    img = W.bernoulli((4096, 4100), p, seed=int(p * 1000))
+    ref, k = O.ccl2d(img)
+    for _ in range(3):
+        lab, n = run2d(ctx, img)
+        assert n == k and np.array_equal(lab, ref)

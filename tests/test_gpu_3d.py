@@ -71,3 +71,15 @@ def test_host_api_and_reference_interface(ctx):
     assert np.array_equal(lab2, ref)
     with pytest.raises(ValueError):
         be.make_labeler("bleq", gpu=True, three_d=True).Label(vol, coh=be.COH_8)
+
+
+@pytest.mark.parametrize("p", [0.1, 0.12, 0.3])
+def test_large_volume_repeated(ctx, p):
+    """Large volumes near the 26-connectivity percolation threshold, labeled three times: each run
+    must equal the oracle (catches schedule-dependent races)."""
+    from labeling_b200 import workloads as W
+    vol = W.bernoulli((384, 384, 320), p, seed=int(p * 1000))
+    ref, k = O.ccl3d(vol)
+    for _ in range(3):
+        lab, n = run3d(ctx, vol)
+        assert n == k and np.array_equal(lab, ref)
