@@ -72,6 +72,25 @@ __device__ __forceinline__ bool perim_pos(int p, int nbr, int nbc, int &r, int &
     return r < nbr;
 }
 
+// Nibble-packed mask words: nibble k = mask of block k; nb_bN gives bit N of every nibble at
+// bit 4k, so block-wise predicates of 8 blocks are a few bitwise operations.
+__device__ __forceinline__ uint32_t nb_b0(uint32_t x) { return x & 0x11111111u; }
+__device__ __forceinline__ uint32_t nb_b1(uint32_t x) { return (x >> 1) & 0x11111111u; }
+__device__ __forceinline__ uint32_t nb_b2(uint32_t x) { return (x >> 2) & 0x11111111u; }
+__device__ __forceinline__ uint32_t nb_b3(uint32_t x) { return (x >> 3) & 0x11111111u; }
+__device__ __forceinline__ uint32_t nb_lft(uint32_t x) { return nb_b0(x) | nb_b2(x); }
+__device__ __forceinline__ uint32_t nb_rgt(uint32_t x) { return nb_b1(x) | nb_b3(x); }
+
+// Four bytes (each < 16) -> four nibbles.
+__device__ __forceinline__ uint32_t bytes_to_nibbles(uint32_t x)
+{
+    x = (x | (x >> 4)) & 0x00FF00FFu;
+    return (x | (x >> 8)) & 0xFFFFu;
+}
+
+// Out-of-line merge keeps the kernel's code small (the merge loop is rare after the skip rules).
+__device__ __noinline__ void merge_blocks(uint32_t *P, uint32_t a, uint32_t b) { smerge(P, a, b); }
+
 __device__ __forceinline__ uint32_t nib2byte(uint32_t x)
 {
     x &= 0xFFFFu;
@@ -85,7 +104,7 @@ __device__ __forceinline__ uint32_t nib2byte(uint32_t x)
 // ---------------------------------------------------------------------------------------------
 // Tile-local labeling.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(K1_NT) k_tile_local_2d(ImgList2D L, Work w)
+__global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
 {
     __shared__ uint32_t P[2 * NBLK];
     __shared__ __align__(16) uint8_t M[NBLK];
@@ -157,43 +176,55 @@ __global__ void __launch_bounds__(K1_NT) k_tile_local_2d(ImgList2D L, Work w)
         }
         __syncthreads();
 
-        // Phase B: merges with the block to the left (across groups) and the row above.
+        // Phase B: merges with the block to the left (across groups) and the row above, decided
+        // for the 8 blocks of a group at once on nibble-packed masks (bit 4k = block k).
 #pragma unroll
         for (int i = 0; i < ITEMS / K1_NT; ++i) {
             const int it = tid + i * K1_NT, r = it / GROUPS, g = it % GROUPS;
             const uint32_t ms = masks[i];
             if (!ms) continue;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t m = (ms >> (4 * k)) & 15u;
-                if (!m) continue;
-                const int c = 8 * g + k;
-                const uint32_t s = slot_of(r, c, m);
-                const uint32_t ml = k > 0 ? (ms >> (4 * (k - 1))) & 15u : (c > 0 ? M[r * TBW + c - 1] : 0u);
-                const bool hcl = hconn(ml, m);
-                if (k == 0 && hcl) smerge(P, s, slot_of(r, c - 1, ml));
-                if (r == 0) continue;
-                const uint8_t *U = &M[(r - 1) * TBW];
-                const uint32_t up = U[c], upl = c > 0 ? U[c - 1] : 0u, upr = c + 1 < TBW ? U[c + 1] : 0u;
-                bool cN = (m & 3u) && (up & 0xCu);
-                bool cNW = (m & 1u) && (upl & 8u);
-                bool cNE = (m & 2u) && (upr & 4u);
-                if (hcl) {   // the left block is in this block's run and already covers these
-                    if ((ml & 3u) && (upl & 0xCu)) cNW = false;
-                    if ((ml & 2u) && (up & 4u)) cN = false;
-                }
-                if (cN) {    // upper blocks joined horizontally to `up` come with it
-                    if (hconn(upl, up)) cNW = false;
-                    if (hconn(up, upr)) cNE = false;
-                }
-                if (cN) smerge(P, s, slot_of(r - 1, c, up));
-                if (cNW) smerge(P, s, slot_of(r - 1, c - 1, upl));
-                if (cNE) smerge(P, s, slot_of(r - 1, c + 1, upr));
+            const int c0 = 8 * g;
+            const uint32_t ML = c0 > 0 ? M[r * TBW + c0 - 1] : 0u;
+            const uint32_t hcl = nb_lft(ms) & ((nb_rgt(ms) << 4) | nb_rgt(ML));
+            if (hcl & 1u) merge_blocks(P, slot_of(r, c0, ms & 15u), slot_of(r, c0 - 1, ML));
+            if (r == 0) continue;
+            const uint8_t *Urow = &M[(r - 1) * TBW];
+            const uint2 ub = *reinterpret_cast<const uint2 *>(Urow + c0);
+            const uint32_t U = bytes_to_nibbles(ub.x) | (bytes_to_nibbles(ub.y) << 16);
+            const uint32_t UL = c0 > 0 ? Urow[c0 - 1] : 0u;
+            const uint32_t UR = c0 + 8 < TBW ? Urow[c0 + 8] : 0u;
+            const uint32_t top = nb_b0(ms) | nb_b1(ms);
+            const uint32_t uBL = nb_b2(U), uBR = nb_b3(U), uB = uBL | uBR;
+            uint32_t cN = top & uB;
+            uint32_t cNW = nb_b0(ms) & ((uBR << 4) | nb_b3(UL));
+            uint32_t cNE = nb_b1(ms) & ((uBL >> 4) | (nb_b2(UR) << 28));
+            // The left block of the same run already reaches these upper blocks.
+            const uint32_t leftN = ((top << 4) | nb_b0(ML) | nb_b1(ML)) & ((uB << 4) | nb_b2(UL) | nb_b3(UL));
+            const uint32_t leftNE = ((nb_b1(ms) << 4) | nb_b1(ML)) & uBL;
+            cNW &= ~(hcl & leftN);
+            cN &= ~(hcl & leftNE);
+            // Upper neighbours joined horizontally to the block above come with it.
+            const uint32_t uL = nb_lft(U), uR = nb_rgt(U);
+            cNW &= ~(cN & (((uR << 4) | nb_rgt(UL)) & uL));
+            cNE &= ~(cN & (uR & ((uL >> 4) | (nb_lft(UR) << 28))));
+            uint32_t todo = cN | cNW | cNE;
+            while (todo) {
+                const int k = (__ffs(todo) - 1) >> 2;
+                const uint32_t bit = 1u << (4 * k);
+                todo &= ~bit;
+                const int c = c0 + k;
+                const uint32_t sl = slot_of(r, c, (ms >> (4 * k)) & 15u);
+                if (cN & bit) merge_blocks(P, sl, slot_of(r - 1, c, (U >> (4 * k)) & 15u));
+                if (cNW & bit)
+                    merge_blocks(P, sl, slot_of(r - 1, c - 1, k ? (U >> (4 * k - 4)) & 15u : UL));
+                if (cNE & bit)
+                    merge_blocks(P, sl, slot_of(r - 1, c + 1, k < 7 ? (U >> (4 * k + 4)) & 15u : UR));
             }
         }
         __syncthreads();
 
-        // Phase C: flatten, write tile-local labels, mark roots.
+        // Phase C: resolve each block's root (read-only: all merges are done), write tile-local
+        // labels, mark roots.
 #pragma unroll
         for (int i = 0; i < ITEMS / K1_NT; ++i) {
             const int it = tid + i * K1_NT, r = it / GROUPS, g = it % GROUPS;
@@ -207,7 +238,6 @@ __global__ void __launch_bounds__(K1_NT) k_tile_local_2d(ImgList2D L, Work w)
                 const int c = 8 * g + k;
                 const uint32_t s = slot_of(r, c, m);
                 const uint32_t root = sfind_ro(P, s);
-                P[s] = root;
                 const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
                 e[k] = (m << 12) | rb;
                 if (root == s) {
@@ -236,7 +266,7 @@ __global__ void __launch_bounds__(K1_NT) k_tile_local_2d(ImgList2D L, Work w)
             if (!perim_pos(p, nbr, nbc, r, c)) continue;
             const uint32_t m = M[r * TBW + c];
             if (!m) continue;
-            const uint32_t root = P[slot_of(r, c, m)];
+            const uint32_t root = sfind_ro(P, slot_of(r, c, m));
             const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
             atomicOr(&BF[rb >> 5], 1u << (rb & 31));
         }
@@ -273,7 +303,7 @@ __global__ void __launch_bounds__(K1_NT) k_tile_local_2d(ImgList2D L, Work w)
             if (perim_pos(p, nbr, nbc, r, c)) {
                 const uint32_t m = M[r * TBW + c];
                 if (m) {
-                    const uint32_t root = P[slot_of(r, c, m)];
+                    const uint32_t root = sfind_ro(P, slot_of(r, c, m));
                     const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
                     const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
                     ent = uint16_t((j << 4) | m);

@@ -70,6 +70,20 @@ __device__ __forceinline__ bool bconn(uint32_t ma, uint32_t mb, int dx, int dy, 
 
 __device__ __forceinline__ int blk(int b0, int b1, int b2) { return (b0 * TB1 + b1) * TB2 + b2; }
 
+// Byte-packed mask words: byte k = mask of block k.  nzb gives bit 8k = (byte k != 0);
+// rep8 repeats a byte selector in all eight bytes.
+__device__ __forceinline__ uint64_t nzb(uint64_t x)
+{
+    x |= x >> 4;
+    x |= x >> 2;
+    x |= x >> 1;
+    return x & 0x0101010101010101ull;
+}
+__device__ __forceinline__ uint64_t rep8(uint32_t sel) { return uint64_t(sel) * 0x0101010101010101ull; }
+
+// Out-of-line merge keeps the kernel's code small.
+__device__ __noinline__ void merge_blocks3(uint32_t *P, uint32_t a, uint32_t b) { smerge(P, a, b); }
+
 // Tile-local key of the first voxel of a block.
 __device__ __forceinline__ uint32_t local_key(int b, uint32_t m)
 {
@@ -165,7 +179,7 @@ __device__ __forceinline__ bool perim_pos3(int p, const TileGeo &g, int &f, int 
 // ---------------------------------------------------------------------------------------------
 // Tile-local labeling.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
+__global__ void __launch_bounds__(NT, 4) k_tile_local_3d(ImgList3D L, Work w)
 {
     __shared__ uint32_t P[NBLK];
     __shared__ uint32_t KM[NBLK];
@@ -232,43 +246,64 @@ __global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
         }
         __syncthreads();
 
-        // Phase B: merges with the 13 preceding neighbours inside the tile.
+        // Phase B: merges with the 13 preceding neighbours inside the tile, decided for the 8
+        // blocks of a group at once on byte-packed masks (bit 8k = block k): the 12 neighbours
+        // in the four preceding rows (d0-1, d1-1 / d0-1, d1 / d0-1, d1+1 / d0, d1-1) and, at the
+        // group's first block, the block before it along d2.
 #pragma unroll
         for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
             const int it = tid + it_i * NT;
             const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
             const uint64_t ms = masks[it_i];
             if (!ms) continue;
+            const int bb = blk(b0, b1, 8 * zg);
+            const uint64_t ML = zg > 0 ? M[bb - 1] : 0u;
+            // hz: block k is joined along d2 to block k-1 (same run)
+            const uint64_t hz = nzb(ms & rep8(side_sel(0, 0, -1))) &
+                                nzb(((ms << 8) | ML) & rep8(side_sel(0, 0, 1)));
+            if (hz & 1u) merge_blocks3(P, bb, bb - 1);
 #pragma unroll 1
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
-                if (!m) continue;
-                const int b2 = 8 * zg + k;
-                const int b = blk(b0, b1, b2);
-                if (k == 0 && b2 > 0) {
-                    const uint32_t mz = M[b - 1];
-                    if (bconn(m, mz, 0, 0, -1)) smerge(P, b, b - 1);
+            for (int row = 0; row < 4; ++row) {
+                const int dx = row < 3 ? -1 : 0, dy = row < 3 ? row - 1 : -1;
+                const int n0 = b0 + dx, n1 = b1 + dy;
+                if (n0 < 0 || n1 < 0 || n1 >= TB1) continue;
+                const int nb0 = blk(n0, n1, 8 * zg);
+                const uint2 nv = *reinterpret_cast<const uint2 *>(&M[nb0]);
+                const uint64_t N = (uint64_t(nv.y) << 32) | nv.x;
+                const uint64_t NL = zg > 0 ? M[nb0 - 1] : 0u;
+                const uint64_t NR = 8 * zg + 8 < TB2 ? M[nb0 + 8] : 0u;
+                if (!(N | NL | NR)) continue;
+                uint64_t c[3];
+#pragma unroll
+                for (int dz = -1; dz <= 1; ++dz) {
+                    const uint64_t Ns = dz < 0 ? (N << 8) | NL : dz > 0 ? (N >> 8) | (NR << 56) : N;
+                    c[dz + 1] = nzb(ms & rep8(side_sel(dx, dy, dz))) & nzb(Ns & rep8(side_sel(-dx, -dy, -dz)));
                 }
-                for (int dx = -1; dx <= 0; ++dx) {
-                    if (b0 + dx < 0) continue;
-                    for (int dy = -1; dy <= 1; ++dy) {
-                        if (dx == 0 && dy >= 0) break;
-                        const int y1 = b1 + dy;
-                        if (y1 < 0 || y1 >= TB1) continue;
-                        for (int dz = -1; dz <= 1; ++dz) {
-                            const int z2 = b2 + dz;
-                            if (z2 < 0 || z2 >= TB2) continue;
-                            const int nbk = blk(b0 + dx, y1, z2);
-                            const uint32_t mn = M[nbk];
-                            if (mn && bconn(m, mn, dx, dy, dz)) smerge(P, b, nbk);
-                        }
-                    }
+                // The previous block of the run already reaches these blocks of row N.
+                c[0] &= ~(hz & (c[1] << 8));
+                c[1] &= ~(hz & (c[2] << 8));
+                // Blocks of row N joined along d2 to the one reached with dz = 0 come with it.
+                const uint64_t hzN = nzb(N & rep8(side_sel(0, 0, -1))) &
+                                     nzb(((N << 8) | NL) & rep8(side_sel(0, 0, 1)));
+                const uint64_t hzN1 = (hzN >> 8) |
+                                      (uint64_t((NR & side_sel(0, 0, -1)) && ((N >> 56) & side_sel(0, 0, 1))) << 56);
+                c[0] &= ~(c[1] & hzN);
+                c[2] &= ~(c[1] & hzN1);
+                uint64_t todo = c[0] | c[1] | c[2];
+                while (todo) {
+                    const int k = (__ffsll(todo) - 1) >> 3;
+                    const uint64_t bit = uint64_t(1) << (8 * k);
+                    todo &= ~bit;
+                    if (c[0] & bit) merge_blocks3(P, bb + k, nb0 + k - 1);
+                    if (c[1] & bit) merge_blocks3(P, bb + k, nb0 + k);
+                    if (c[2] & bit) merge_blocks3(P, bb + k, nb0 + k + 1);
                 }
             }
         }
         __syncthreads();
 
-        // Phase C: flatten and per-component first-voxel key.
+        // Phase C: roots (read-only finds: all merges are done) and per-component first-voxel key.
+        uint16_t roots[ITEMS / NT][8];
 #pragma unroll
         for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
             const int it = tid + it_i * NT;
@@ -280,7 +315,7 @@ __global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
                 if (!m) continue;
                 const int b = blk(b0, b1, 8 * zg + k);
                 const uint32_t root = sfind_ro(P, b);
-                P[b] = root;
+                roots[it_i][k] = uint16_t(root);
                 atomicMin(&KM[root], local_key(b, m));
             }
         }
@@ -298,7 +333,7 @@ __global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
                 e[k] = 0;
                 if (!m) continue;
                 const int b = bb + k;
-                const uint32_t root = P[b];
+                const uint32_t root = roots[it_i][k];
                 if (root == uint32_t(b)) {
                     const uint32_t key = KM[b];
                     e[k] = (m << 24) | ROOT_FLAG | key;
@@ -330,7 +365,7 @@ __global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
             if (!perim_pos3(p, g, f, b0, b1, b2)) continue;
             const int b = blk(b0, b1, b2);
             if (!M[b]) continue;
-            const uint32_t rb = P[b];
+            const uint32_t rb = sfind_ro(P, b);
             atomicOr(&BF[rb >> 5], 1u << (rb & 31));
         }
         __syncthreads();
@@ -367,7 +402,7 @@ __global__ void __launch_bounds__(NT) k_tile_local_3d(ImgList3D L, Work w)
                 const int b = blk(b0, b1, b2);
                 const uint32_t m = M[b];
                 if (m) {
-                    const uint32_t rb = P[b];
+                    const uint32_t rb = sfind_ro(P, b);
                     const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
                     ent = uint16_t((j << 4) | face_bits(m, f));
                 }
