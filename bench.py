@@ -211,6 +211,7 @@ def bench_ours(args, rank, world, local_rank):
         ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         stage_ms = np.zeros(len(stages))
+        per_stage = {}
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
@@ -224,6 +225,7 @@ def bench_ours(args, rank, world, local_rank):
                 ev1[s].record(stream)
                 st = ctx.stage_times()
                 stage_ms += np.array(st[:len(stages)])
+                per_stage.setdefault(inputs[i][0], []).append(st[:len(stages)])
                 px_done += npx[i]
             torch.cuda.synchronize()
         ctx.set_stage_timing(False)
@@ -303,6 +305,7 @@ def bench_ours(args, rank, world, local_rank):
         "gpu_launches": 5 * steps, "clocks": clocks,
         "components": {n: c for (n, _), c in zip(inputs, counts)},
         "per_image_ms": per_image,
+        "per_image_stage_ms": {k: [round(float(x), 4) for x in np.mean(v, axis=0)] for k, v in per_stage.items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         budget = 20.0

@@ -41,6 +41,7 @@ Geometry geometry_2d()
 {
     Geometry g;
     g.lab_bytes_per_tile = size_t(T2_TBW) * T2_TBH * sizeof(uint16_t);
+    g.rbits_bytes_per_tile = size_t(2 * T2_TBH) * (2 * T2_TBW / 32) * sizeof(uint32_t);
     g.nperim = T2_NPERIM;
     g.maxb = T2_MAXB;
     return g;
@@ -50,6 +51,7 @@ Geometry geometry_3d()
 {
     Geometry g;
     g.lab_bytes_per_tile = size_t(T3_NBLK) * sizeof(uint32_t);
+    g.rbits_bytes_per_tile = 0;
     g.nperim = T3_NPERIM;
     g.maxb = T3_MAXB;
     return g;
@@ -70,6 +72,7 @@ size_t layout_work(const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_img
     Work t{};
     t.lab = take(size_t(n_tiles) * g.lab_bytes_per_tile);
     t.perim = reinterpret_cast<uint16_t *>(take(size_t(n_tiles) * g.nperim * sizeof(uint16_t)));
+    t.rbits = reinterpret_cast<uint32_t *>(take(size_t(n_tiles) * g.rbits_bytes_per_tile));
     t.nb = reinterpret_cast<uint32_t *>(take(size_t(n_tiles) * sizeof(uint32_t)));
     t.gp = reinterpret_cast<uint32_t *>(take(nodes * sizeof(uint32_t)));
     t.nkey = reinterpret_cast<uint32_t *>(take(nodes * sizeof(uint32_t)));

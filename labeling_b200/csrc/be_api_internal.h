@@ -1,5 +1,6 @@
 // be_api_internal.h -- host-side state behind the C ABI (not part of the public interface).
 #pragma once
+#include "be.h"
 #include "be_common.cuh"
 
 #include <cuda_runtime.h>
@@ -12,6 +13,7 @@ constexpr int kQueueWords = 16;   // work-queue counters per workspace (one per 
 // Per-tile sizes of a pipeline's workspace.
 struct Geometry {
     size_t lab_bytes_per_tile;
+    size_t rbits_bytes_per_tile;
     int nperim;
     int maxb;
 };

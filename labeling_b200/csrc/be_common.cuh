@@ -67,6 +67,7 @@ struct Work {
     uint16_t *nlrank;     // per node: rank of the root among the tile's roots in its segment
     uint16_t *nroot;      // per node: tile-local block index of the node's root block
     uint32_t *grank;      // per node that stays a root: rank among global roots in its segment
+    uint32_t *rbits;      // per tile: bitmap of the first pixels of the tile's components
     uint8_t *segcnt;      // per segment: number of component roots (uint8, word-padded)
     uint32_t *segpref;    // per segment + 1: exclusive prefix of segcnt over the launch
     uint32_t *chunksum;   // per scan chunk: sum of segcnt
@@ -161,6 +162,20 @@ __device__ __forceinline__ uint32_t sfind_ro(const uint32_t *P, uint32_t a)
     return a;
 }
 
+// Root of `a` after all merges, pointing every entry on the path straight at it.  Safe while
+// other threads do the same: all of them store the same final root into shared entries.
+__device__ __forceinline__ uint32_t sflatten(uint32_t *P, uint32_t a)
+{
+    const uint32_t r = sfind_ro(P, a);
+    uint32_t x = a;
+    while (x != r) {
+        const uint32_t nx = P[x];
+        P[x] = r;
+        x = nx;
+    }
+    return r;
+}
+
 // Merge of two shared-memory union-find trees that keeps the smaller index as the root
 // (the atomicMin formulation of Playne & Hawick's union-find, safe under concurrent merges).
 __device__ __forceinline__ void smerge(uint32_t *P, uint32_t a, uint32_t b)
@@ -179,6 +194,97 @@ __device__ __forceinline__ void smerge(uint32_t *P, uint32_t a, uint32_t b)
             a = old;
         }
     }
+}
+
+// ---- 16-bit shared-memory union-find (indices < 65536) ---------------------------------------
+// Same algorithm as sfind / smerge on uint16 parents, which halves the footprint.  The atomic
+// minimum is a compare-and-swap on the aligned 32-bit word holding the entry; plain 16-bit stores
+// to either half of that word make the CAS retry, which is all the correctness needs.
+__device__ __forceinline__ uint32_t atomic_min_u16(uint16_t *addr, uint32_t val)
+{
+    uint32_t *word = reinterpret_cast<uint32_t *>(reinterpret_cast<uintptr_t>(addr) & ~uintptr_t(3));
+    const uint32_t sh = (reinterpret_cast<uintptr_t>(addr) & 2) * 8;
+    uint32_t old = *reinterpret_cast<volatile uint32_t *>(word);
+    for (;;) {
+        const uint32_t cur = (old >> sh) & 0xFFFFu;
+        if (val >= cur) return cur;
+        const uint32_t nv = (old & ~(0xFFFFu << sh)) | (val << sh);
+        const uint32_t seen = atomicCAS(word, old, nv);
+        if (seen == old) return cur;
+        old = seen;
+    }
+}
+
+__device__ __forceinline__ uint32_t sfind16(uint16_t *P, uint32_t a)
+{
+    uint32_t p = P[a];
+    while (p != a) {
+        const uint32_t g = P[p];
+        if (g != p) P[a] = uint16_t(g);
+        a = p;
+        p = g;
+    }
+    return a;
+}
+
+__device__ __forceinline__ uint32_t sfind16_ro(const uint16_t *P, uint32_t a)
+{
+    uint32_t p = P[a];
+    while (p != a) {
+        a = p;
+        p = P[a];
+    }
+    return a;
+}
+
+// Root of `a` after all merges, pointing every entry on the path straight at it.  Safe while
+// other threads do the same: all of them store the same final root into shared entries.
+__device__ __forceinline__ uint32_t sflatten16(uint16_t *P, uint32_t a)
+{
+    const uint32_t r = sfind16_ro(P, a);
+    uint32_t x = a;
+    while (x != r) {
+        const uint32_t nx = P[x];
+        P[x] = uint16_t(r);
+        x = nx;
+    }
+    return r;
+}
+
+__device__ __forceinline__ void smerge16(uint16_t *P, uint32_t a, uint32_t b)
+{
+    for (;;) {
+        a = sfind16(P, a);
+        b = sfind16(P, b);
+        if (a == b) return;
+        if (a < b) {
+            const uint32_t old = atomic_min_u16(&P[b], a);
+            if (old == b) return;
+            b = old;
+        } else {
+            const uint32_t old = atomic_min_u16(&P[a], b);
+            if (old == a) return;
+            a = old;
+        }
+    }
+}
+
+// Appends this lane's `n` merge pairs to a shared queue with one atomic per warp; returns the
+// lane's first position (positions >= capacity mean the queue is full for those pairs).
+__device__ __forceinline__ uint32_t warp_reserve(uint32_t *count, uint32_t n)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    uint32_t base = 0;
+    if (lane == 31 && total) base = atomicAdd(count, total);
+    base = __shfl_sync(0xFFFFFFFFu, base, 31);
+    return base + incl - n;
 }
 
 // Global union-find find with path halving.  Only non-root entries are rewritten and only with an

@@ -40,6 +40,7 @@ constexpr int MAXB = T2_MAXB;                      // nodes per tile
 constexpr int K1_NT = 256;
 constexpr int ITEMS = NBLK / 8;                    // 8-block row groups per tile
 constexpr int GROUPS = TBW / 8;                    // groups per block row
+constexpr int MQCAP = 2048;                        // merge-queue capacity (pairs per tile)
 
 static_assert(NBLK <= 4096, "tile-local block index must fit 12 bits");
 static_assert(MAXB < 4096, "node index must fit 12 bits");
@@ -88,9 +89,6 @@ __device__ __forceinline__ uint32_t bytes_to_nibbles(uint32_t x)
     return (x | (x >> 8)) & 0xFFFFu;
 }
 
-// Out-of-line merge keeps the kernel's code small (the merge loop is rare after the skip rules).
-__device__ __noinline__ void merge_blocks(uint32_t *P, uint32_t a, uint32_t b) { smerge(P, a, b); }
-
 __device__ __forceinline__ uint32_t nib2byte(uint32_t x)
 {
     x &= 0xFFFFu;
@@ -111,6 +109,8 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
     __shared__ uint32_t RB[TH][TW / 32];
     __shared__ uint32_t BF[NBLK / 32];
     __shared__ uint32_t BP[NBLK / 32];
+    __shared__ uint32_t MQ[MQCAP];          // merge queue: (slot_a << 16) | slot_b
+    __shared__ uint32_t mqn[2];
     __shared__ uint32_t tmp[K1_NT / 32 + 1];
     __shared__ uint32_t qslot;
 
@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
 
         for (int i = tid; i < TH * (TW / 32); i += K1_NT) (&RB[0][0])[i] = 0;
         if (tid < NBLK / 32) BF[tid] = 0;
+        if (tid < 2) mqn[tid] = 0;
 
         // Phase A: load pixels, build block masks, seed the union-find with horizontal runs.
         uint32_t masks[ITEMS / K1_NT];
@@ -155,58 +156,121 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
             const uint32_t ms = pairs_to_nibbles(top) | (pairs_to_nibbles(bot) << 2);
             masks[i] = ms;
             *reinterpret_cast<uint2 *>(&M[r * TBW + 8 * g]) = make_uint2(nib2byte(ms), nib2byte(ms >> 16));
-            // Horizontal runs inside the group: every block points at the run's smallest slot.
+            // Horizontal runs: every block points at its run's smallest slot.  Within the group
+            // a prefix minimum finds each run part's minimum; runs that cross group borders are
+            // joined with segmented minimum scans over the 16 groups of the block row (one
+            // half-warp), so no merge is needed for horizontal links.
             uint32_t pm[8];
+            bool inf[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 const uint32_t m = (ms >> (4 * k)) & 15u;
                 const uint32_t s = slot_of(r, 8 * g + k, m);
                 const bool hc = k > 0 && hconn((ms >> (4 * (k - 1))) & 15u, m);
                 pm[k] = hc ? min(pm[k - 1], s) : s;
+                inf[k] = k == 0 ? (m != 0) : (inf[k - 1] && hc);
             }
-            uint32_t run = 0;
+            const uint32_t m0 = ms & 15u, m7 = ms >> 28;
+            const uint32_t prev_ms = __shfl_up_sync(0xFFFFFFFFu, ms, 1, 16);
+            const bool linkL = g > 0 && hconn(prev_ms >> 28, m0);
+            const bool linkR = __shfl_down_sync(0xFFFFFFFFu, uint32_t(linkL), 1, 16) && g + 1 < GROUPS;
+            const bool single = inf[7];
+            // first_min: minimum of the run part holding block 0 (found by the backward pass).
+            uint32_t run = kNone, first_min = kNone;
+            uint32_t part[8];
 #pragma unroll
             for (int k = 7; k >= 0; --k) {
                 const uint32_t m = (ms >> (4 * k)) & 15u;
-                if (!m) continue;
                 const bool last = (k == 7) || !hconn(m, (ms >> (4 * (k + 1))) & 15u);
                 if (last) run = pm[k];
-                P[slot_of(r, 8 * g + k, m)] = run;
+                part[k] = run;
+            }
+            first_min = m0 ? part[0] : kNone;
+            const uint32_t last_min = m7 ? pm[7] : kNone;
+            // Left-to-right: minimum of the run entering from the left.
+            uint32_t fv = last_min;
+            uint32_t ff = !(single && linkL);
+#pragma unroll
+            for (int o = 1; o < 16; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, fv, o, 16);
+                const uint32_t f = __shfl_up_sync(0xFFFFFFFFu, ff, o, 16);
+                if (g >= o && !ff) { fv = min(fv, v); ff |= f; }
+            }
+            const uint32_t fprev = __shfl_up_sync(0xFFFFFFFFu, fv, 1, 16);
+            const uint32_t fromL = linkL ? fprev : kNone;
+            // Right-to-left: minimum of the run leaving to the right.
+            uint32_t bv = first_min;
+            uint32_t bf = !(single && linkR);
+#pragma unroll
+            for (int o = 1; o < 16; o <<= 1) {
+                const uint32_t v = __shfl_down_sync(0xFFFFFFFFu, bv, o, 16);
+                const uint32_t f = __shfl_down_sync(0xFFFFFFFFu, bf, o, 16);
+                if (g + o < GROUPS && !bf) { bv = min(bv, v); bf |= f; }
+            }
+            const uint32_t bnext = __shfl_down_sync(0xFFFFFFFFu, bv, 1, 16);
+            const uint32_t fromR = linkR ? bnext : kNone;
+            bool inl = m7 != 0;
+#pragma unroll
+            for (int k = 7; k >= 0; --k) {
+                const uint32_t m = (ms >> (4 * k)) & 15u;
+                if (k < 7) inl = inl && hconn(m, (ms >> (4 * (k + 1))) & 15u);
+                if (!m) continue;
+                uint32_t v = part[k];
+                if (inf[k]) v = min(v, fromL);
+                if (inl) v = min(v, fromR);
+                P[slot_of(r, 8 * g + k, m)] = v;
             }
         }
         __syncthreads();
 
-        // Phase B: merges with the block to the left (across groups) and the row above, decided
-        // for the 8 blocks of a group at once on nibble-packed masks (bit 4k = block k).
+        // Phase B: the links to the row above, decided for the 8 blocks of a group at once on
+        // nibble-packed masks (bit 4k = block k), are queued in shared memory and then merged
+        // with every lane busy (one round per item, so the queue rarely overflows).
 #pragma unroll
         for (int i = 0; i < ITEMS / K1_NT; ++i) {
             const int it = tid + i * K1_NT, r = it / GROUPS, g = it % GROUPS;
             const uint32_t ms = masks[i];
-            if (!ms) continue;
             const int c0 = 8 * g;
-            const uint32_t ML = c0 > 0 ? M[r * TBW + c0 - 1] : 0u;
-            const uint32_t hcl = nb_lft(ms) & ((nb_rgt(ms) << 4) | nb_rgt(ML));
-            if (hcl & 1u) merge_blocks(P, slot_of(r, c0, ms & 15u), slot_of(r, c0 - 1, ML));
-            if (r == 0) continue;
-            const uint8_t *Urow = &M[(r - 1) * TBW];
-            const uint2 ub = *reinterpret_cast<const uint2 *>(Urow + c0);
-            const uint32_t U = bytes_to_nibbles(ub.x) | (bytes_to_nibbles(ub.y) << 16);
-            const uint32_t UL = c0 > 0 ? Urow[c0 - 1] : 0u;
-            const uint32_t UR = c0 + 8 < TBW ? Urow[c0 + 8] : 0u;
-            const uint32_t top = nb_b0(ms) | nb_b1(ms);
-            const uint32_t uBL = nb_b2(U), uBR = nb_b3(U), uB = uBL | uBR;
-            uint32_t cN = top & uB;
-            uint32_t cNW = nb_b0(ms) & ((uBR << 4) | nb_b3(UL));
-            uint32_t cNE = nb_b1(ms) & ((uBL >> 4) | (nb_b2(UR) << 28));
-            // The left block of the same run already reaches these upper blocks.
-            const uint32_t leftN = ((top << 4) | nb_b0(ML) | nb_b1(ML)) & ((uB << 4) | nb_b2(UL) | nb_b3(UL));
-            const uint32_t leftNE = ((nb_b1(ms) << 4) | nb_b1(ML)) & uBL;
-            cNW &= ~(hcl & leftN);
-            cN &= ~(hcl & leftNE);
-            // Upper neighbours joined horizontally to the block above come with it.
-            const uint32_t uL = nb_lft(U), uR = nb_rgt(U);
-            cNW &= ~(cN & (((uR << 4) | nb_rgt(UL)) & uL));
-            cNE &= ~(cN & (uR & ((uL >> 4) | (nb_lft(UR) << 28))));
+            uint32_t *qn = &mqn[i];
+            uint32_t hcl = 0, cN = 0, cNW = 0, cNE = 0, U = 0, UL = 0, UR = 0, ML = 0;
+            if (ms) {
+                ML = c0 > 0 ? M[r * TBW + c0 - 1] : 0u;
+                hcl = nb_lft(ms) & ((nb_rgt(ms) << 4) | nb_rgt(ML));
+                if (r > 0) {
+                    const uint8_t *Urow = &M[(r - 1) * TBW];
+                    const uint2 ub = *reinterpret_cast<const uint2 *>(Urow + c0);
+                    U = bytes_to_nibbles(ub.x) | (bytes_to_nibbles(ub.y) << 16);
+                    UL = c0 > 0 ? Urow[c0 - 1] : 0u;
+                    UR = c0 + 8 < TBW ? Urow[c0 + 8] : 0u;
+                    const uint32_t top = nb_b0(ms) | nb_b1(ms);
+                    const uint32_t uBL = nb_b2(U), uBR = nb_b3(U), uB = uBL | uBR;
+                    const uint32_t rawN = top & uB;
+                    cN = rawN;
+                    cNW = nb_b0(ms) & ((uBR << 4) | nb_b3(UL));
+                    cNE = nb_b1(ms) & ((uBL >> 4) | (nb_b2(UR) << 28));
+                    // Skip rules.  A link may be skipped when its two blocks are already joined
+                    // through links that are made or are themselves skipped for a reason further
+                    // left; every chain of reasons runs leftward along the run and ends at a
+                    // link that is made.
+                    // (1) The left block of the same run touches the same upper block.
+                    const uint32_t leftN = ((top << 4) | nb_b0(ML) | nb_b1(ML)) & ((uB << 4) | nb_b2(UL) | nb_b3(UL));
+                    const uint32_t leftNE = ((nb_b1(ms) << 4) | nb_b1(ML)) & uBL;
+                    cNW &= ~(hcl & leftN);
+                    cN &= ~(hcl & leftNE);
+                    // (2) The upper diagonal block is joined horizontally to the block straight
+                    //     above, which this block touches.
+                    const uint32_t uL = nb_lft(U), uR = nb_rgt(U);
+                    cNW &= ~(rawN & (((uR << 4) | nb_rgt(UL)) & uL));
+                    cNE &= ~(rawN & (uR & ((uL >> 4) | (nb_lft(UR) << 28))));
+                }
+            }
+            const uint32_t n = __popc(cN) + __popc(cNW) + __popc(cNE);
+            uint32_t pos = warp_reserve(qn, n);
+            auto push = [&](uint32_t a, uint32_t b) {
+                if (pos < MQCAP) MQ[pos] = (a << 16) | b;
+                else smerge(P, a, b);   // queue full: merge in place
+                ++pos;
+            };
             uint32_t todo = cN | cNW | cNE;
             while (todo) {
                 const int k = (__ffs(todo) - 1) >> 2;
@@ -214,14 +278,15 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
                 todo &= ~bit;
                 const int c = c0 + k;
                 const uint32_t sl = slot_of(r, c, (ms >> (4 * k)) & 15u);
-                if (cN & bit) merge_blocks(P, sl, slot_of(r - 1, c, (U >> (4 * k)) & 15u));
-                if (cNW & bit)
-                    merge_blocks(P, sl, slot_of(r - 1, c - 1, k ? (U >> (4 * k - 4)) & 15u : UL));
-                if (cNE & bit)
-                    merge_blocks(P, sl, slot_of(r - 1, c + 1, k < 7 ? (U >> (4 * k + 4)) & 15u : UR));
+                if (cN & bit) push(sl, slot_of(r - 1, c, (U >> (4 * k)) & 15u));
+                if (cNW & bit) push(sl, slot_of(r - 1, c - 1, k ? (U >> (4 * k - 4)) & 15u : UL));
+                if (cNE & bit) push(sl, slot_of(r - 1, c + 1, k < 7 ? (U >> (4 * k + 4)) & 15u : UR));
             }
+            __syncthreads();
+            const uint32_t nq = min(*qn, uint32_t(MQCAP));
+            for (uint32_t q = tid; q < nq; q += K1_NT) smerge(P, MQ[q] >> 16, MQ[q] & 0xFFFFu);
+            __syncthreads();
         }
-        __syncthreads();
 
         // Phase C: resolve each block's root (read-only: all merges are done), write tile-local
         // labels, mark roots.
@@ -237,7 +302,7 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
                 if (!m) continue;
                 const int c = 8 * g + k;
                 const uint32_t s = slot_of(r, c, m);
-                const uint32_t root = sfind_ro(P, s);
+                const uint32_t root = sflatten(P, s);
                 const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
                 e[k] = (m << 12) | rb;
                 if (root == s) {
@@ -254,20 +319,26 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
         }
         __syncthreads();
 
-        // Phase D: segment counts, border components -> nodes.
+        // Phase D: root bitmap and segment counts out; border components -> nodes.
+        for (int i = tid; i < TH * (TW / 32); i += K1_NT) w.rbits[t * (TH * (TW / 32)) + i] = (&RB[0][0])[i];
         if (tid < TH && tid < nrp) {
             uint32_t cnt = 0;
 #pragma unroll
             for (int k = 0; k < TW / 32; ++k) cnt += __popc(RB[tid][k]);
             w.segcnt[im.seg_base + int64_t(y0 + tid) * im.tiles_x + tx] = uint8_t(cnt);
         }
-        for (int p = tid; p < NPERIM; p += K1_NT) {
+        uint32_t prb[(NPERIM + K1_NT - 1) / K1_NT];   // root block of each border position held
+#pragma unroll
+        for (int i = 0; i < (NPERIM + K1_NT - 1) / K1_NT; ++i) {
+            const int p = tid + i * K1_NT;
             int r, c;
-            if (!perim_pos(p, nbr, nbc, r, c)) continue;
+            prb[i] = kNone;
+            if (p >= NPERIM || !perim_pos(p, nbr, nbc, r, c)) continue;
             const uint32_t m = M[r * TBW + c];
             if (!m) continue;
             const uint32_t root = sfind_ro(P, slot_of(r, c, m));
-            const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
+            const uint32_t rb = (root >> 8) * TBW + (root & (TBW - 1));
+            prb[i] = rb | (m << 16);
             atomicOr(&BF[rb >> 5], 1u << (rb & 31));
         }
         __syncthreads();
@@ -275,18 +346,20 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
         const uint32_t pre = block_exscan<K1_NT>(tid < NBLK / 32 ? __popc(BF[tid]) : 0u, tmp, &nb);
         if (tid < NBLK / 32) BP[tid] = pre;
         __syncthreads();
-        if (tid < NBLK / 32) {
-            uint32_t bits = BF[tid];
-            uint32_t j = pre;
-            while (bits) {
-                const int b = __ffs(bits) - 1;
-                bits &= bits - 1;
-                const uint32_t rb = tid * 32 + b;
-                const uint32_t m = M[rb];
+        // Every border position writes its entry and (redundantly, with identical values) the
+        // record of the node its root belongs to, which spreads the node work over the CTA.
+#pragma unroll
+        for (int i = 0; i < (NPERIM + K1_NT - 1) / K1_NT; ++i) {
+            const int p = tid + i * K1_NT;
+            if (p >= NPERIM) continue;
+            uint16_t ent = 0;
+            if (prb[i] != kNone) {
+                const uint32_t rb = prb[i] & 0xFFFFu, m = prb[i] >> 16;
+                const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
+                ent = uint16_t((j << 4) | m);
                 int dy, dx;
-                first_px(m, dy, dx);
-                const int rr = int(rb) / TBW, cc = int(rb) % TBW;
-                const int y = 2 * rr + dy, x = 2 * cc + dx;
+                first_px(M[rb], dy, dx);
+                const int y = 2 * int(rb / TBW) + dy, x = 2 * int(rb % TBW) + dx;
                 uint32_t rank = __popc(RB[y][x >> 5] & ((1u << (x & 31)) - 1u));
                 for (int k = 0; k < (x >> 5); ++k) rank += __popc(RB[y][k]);
                 const int64_t node = t * MAXB + j;
@@ -294,20 +367,6 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
                 w.nkey[node] = uint32_t(int64_t(y0 + y) * im.cols + (x0 + x));
                 w.nlrank[node] = uint16_t(rank);
                 w.gp[node] = uint32_t(node);
-                ++j;
-            }
-        }
-        for (int p = tid; p < NPERIM; p += K1_NT) {
-            int r, c;
-            uint16_t ent = 0;
-            if (perim_pos(p, nbr, nbc, r, c)) {
-                const uint32_t m = M[r * TBW + c];
-                if (m) {
-                    const uint32_t root = sfind_ro(P, slot_of(r, c, m));
-                    const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
-                    const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
-                    ent = uint16_t((j << 4) | m);
-                }
             }
             w.perim[t * NPERIM + p] = ent;
         }
@@ -457,16 +516,17 @@ __device__ void post_tile_2d(const ImgList2D &L, Work &w, int64_t t)
 // Label resolve and write.
 // ---------------------------------------------------------------------------------------------
 constexpr int K3_NT = 256;
+constexpr int RBWORDS = TH * (TW / 32);   // root-bitmap words per tile (8 per pixel row)
 
 __global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
 {
     __shared__ __align__(16) uint16_t Ls[NBLK];
     __shared__ uint32_t LT[NBLK];
-    __shared__ uint32_t RB[TH][TW / 32];
+    __shared__ uint32_t RB[RBWORDS];
     __shared__ uint32_t segb[TH];
     __shared__ uint32_t qslot;
 
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const uint16_t *lab = reinterpret_cast<const uint16_t *>(w.lab);
     ItemLoop loop{w.queue ? w.queue + 4 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
@@ -475,28 +535,18 @@ __global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
         const int ty = int(lt / im.tiles_x), tx = int(lt - int64_t(ty) * im.tiles_x);
         const int y0 = ty * TH, x0 = tx * TW;
         const int nrp = min(TH, im.rows - y0), ncp = min(TW, im.cols - x0);
-        const int nbr = (nrp + 1) >> 1, nbc = (ncp + 1) >> 1;
         const uint32_t base0 = w.segpref[im.seg_base];
 
         for (int i = tid; i < NBLK / 8; i += K3_NT)
             reinterpret_cast<uint4 *>(Ls)[i] = reinterpret_cast<const uint4 *>(lab + t * NBLK)[i];
-        for (int i = tid; i < TH * (TW / 32); i += K3_NT) (&RB[0][0])[i] = 0;
+        for (int i = tid; i < RBWORDS; i += K3_NT) RB[i] = w.rbits[t * RBWORDS + i];
         if (tid < TH && tid < nrp)
             segb[tid] = w.segpref[im.seg_base + int64_t(y0 + tid) * im.tiles_x + tx] - base0;
         if (lt == 0 && tid == 0)
             w.ncomp[im.index] = int64_t(w.segpref[im.seg_base + int64_t(im.rows) * im.tiles_x] - base0);
         __syncthreads();
 
-        // Roots of this tile.
-        for (int b = tid; b < NBLK; b += K3_NT) {
-            const uint32_t e = Ls[b];
-            if (!(e >> 12) || (e & 0xFFFu) != uint32_t(b)) continue;
-            int dy, dx;
-            first_px(e >> 12, dy, dx);
-            const int y = 2 * (b / TBW) + dy, x = 2 * (b % TBW) + dx;
-            atomicOr(&RB[y][x >> 5], 1u << (x & 31));
-        }
-        __syncthreads();
+        // Border roots linked under another tile's root are not roots any more.
         const uint32_t nb = w.nb[t];
         for (uint32_t j = tid; j < nb; j += K3_NT) {
             const int64_t node = t * MAXB + j;
@@ -505,20 +555,31 @@ __global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
             int dy, dx;
             first_px(Ls[rb] >> 12, dy, dx);
             const int y = 2 * int(rb / TBW) + dy, x = 2 * int(rb % TBW) + dx;
-            atomicAnd(&RB[y][x >> 5], ~(1u << (x & 31)));
+            atomicAnd(&RB[y * (TW / 32) + (x >> 5)], ~(1u << (x & 31)));
         }
         __syncthreads();
-        for (int b = tid; b < NBLK; b += K3_NT) {
-            const uint32_t e = Ls[b];
-            if (!(e >> 12) || (e & 0xFFFu) != uint32_t(b)) continue;
-            int dy, dx;
-            first_px(e >> 12, dy, dx);
-            const int y = 2 * (b / TBW) + dy, x = 2 * (b % TBW) + dx;
-            uint32_t rank = __popc(RB[y][x >> 5] & ((1u << (x & 31)) - 1u));
-            for (int k = 0; k < (x >> 5); ++k) rank += __popc(RB[y][k]);
-            LT[b] = 1u + segb[y] + rank;
+
+        // Surviving roots: rank = roots before it in its row segment.  Eight consecutive lanes
+        // hold the eight words of one pixel row; a shuffle scan gives each word's prefix.
+        for (int i = tid; i < RBWORDS; i += K3_NT) {
+            const uint32_t word = RB[i];
+            uint32_t pre = __popc(word);
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, pre, o);
+                if ((lane & 7) >= o) pre += v;
+            }
+            pre -= __popc(word);
+            const int y = i >> 3, q = i & 7;
+            const uint32_t base = 1u + segb[y] + pre;
+            uint32_t bits = word;
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                const int x = 32 * q + b;
+                LT[(y >> 1) * TBW + (x >> 1)] = base + __popc(word & ((1u << b) - 1u));
+                bits &= bits - 1;
+            }
         }
-        __syncthreads();
         for (uint32_t j = tid; j < nb; j += K3_NT) {
             const int64_t node = t * MAXB + j;
             if (w.gp[node] == uint32_t(node)) continue;
@@ -530,30 +591,33 @@ __global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
         }
         __syncthreads();
 
-        // Output: one int4 (4 pixels of one row) per unit.
+        // Output: one unit = two horizontally adjacent blocks = 4 pixels in each of 2 rows.
         const bool vec_ok = ((reinterpret_cast<uintptr_t>(im.out) | uintptr_t(im.out_pitch * 4)) & 15) == 0;
-        for (int u = tid; u < TH * (TW / 4); u += K3_NT) {
-            const int y = u / (TW / 4), q = u % (TW / 4);
+        for (int u = tid; u < NBLK / 2; u += K3_NT) {
+            const int br = u / (TBW / 2), q = u % (TBW / 2);
+            const int y = 2 * br;
             if (y >= nrp || 4 * q >= ncp) continue;
-            const int br = y >> 1, h = (y & 1) * 2;
-            const uint32_t e0 = Ls[br * TBW + 2 * q];
-            const uint32_t e1 = 2 * q + 1 < nbc ? Ls[br * TBW + 2 * q + 1] : 0u;
+            const uint32_t ee = reinterpret_cast<const uint32_t *>(Ls)[u];
+            const uint32_t e0 = ee & 0xFFFFu, e1 = ee >> 16;
             const uint32_t m0 = e0 >> 12, m1 = e1 >> 12;
-            const uint32_t l0 = m0 ? LT[e0 & 0xFFFu] : 0u, l1 = m1 ? LT[e1 & 0xFFFu] : 0u;
-            int4 v;
-            v.x = ((m0 >> h) & 1u) ? int(l0) : 0;
-            v.y = ((m0 >> (h + 1)) & 1u) ? int(l0) : 0;
-            v.z = ((m1 >> h) & 1u) ? int(l1) : 0;
-            v.w = ((m1 >> (h + 1)) & 1u) ? int(l1) : 0;
+            const int l0 = m0 ? int(LT[e0 & 0xFFFu]) : 0, l1 = m1 ? int(LT[e1 & 0xFFFu]) : 0;
+            int4 a, b;
+            a.x = (m0 & 1u) ? l0 : 0; a.y = (m0 & 2u) ? l0 : 0;
+            a.z = (m1 & 1u) ? l1 : 0; a.w = (m1 & 2u) ? l1 : 0;
+            b.x = (m0 & 4u) ? l0 : 0; b.y = (m0 & 8u) ? l0 : 0;
+            b.z = (m1 & 4u) ? l1 : 0; b.w = (m1 & 8u) ? l1 : 0;
             int32_t *dst = im.out + int64_t(y0 + y) * im.out_pitch + x0 + 4 * q;
+            const bool row2 = y + 1 < nrp;
             if (vec_ok && 4 * q + 4 <= ncp) {
-                __stcs(reinterpret_cast<int4 *>(dst), v);
+                __stcs(reinterpret_cast<int4 *>(dst), a);
+                if (row2) __stcs(reinterpret_cast<int4 *>(dst + im.out_pitch), b);
             } else {
                 const int n = min(4, ncp - 4 * q);
-                dst[0] = v.x;
-                if (n > 1) dst[1] = v.y;
-                if (n > 2) dst[2] = v.z;
-                if (n > 3) dst[3] = v.w;
+                const int va[4] = {a.x, a.y, a.z, a.w}, vb[4] = {b.x, b.y, b.z, b.w};
+                for (int k = 0; k < n; ++k) {
+                    dst[k] = va[k];
+                    if (row2) dst[im.out_pitch + k] = vb[k];
+                }
             }
         }
         __syncthreads();

@@ -279,16 +279,19 @@ __global__ void __launch_bounds__(NT, 4) k_tile_local_3d(ImgList3D L, Work w)
                     const uint64_t Ns = dz < 0 ? (N << 8) | NL : dz > 0 ? (N >> 8) | (NR << 56) : N;
                     c[dz + 1] = nzb(ms & rep8(side_sel(dx, dy, dz))) & nzb(Ns & rep8(side_sel(-dx, -dy, -dz)));
                 }
-                // The previous block of the run already reaches these blocks of row N.
-                c[0] &= ~(hz & (c[1] << 8));
+                // Skip rules (as in the 2D kernel: every chain of reasons runs toward smaller
+                // d2 along the run and ends at a link that is made).
+                // (1) The previous block of the run touches the same block of row N.
+                const uint64_t raw1 = c[1];
+                c[0] &= ~(hz & (raw1 << 8));
                 c[1] &= ~(hz & (c[2] << 8));
-                // Blocks of row N joined along d2 to the one reached with dz = 0 come with it.
+                // (2) Blocks of row N joined along d2 to the block this one touches with dz = 0.
                 const uint64_t hzN = nzb(N & rep8(side_sel(0, 0, -1))) &
                                      nzb(((N << 8) | NL) & rep8(side_sel(0, 0, 1)));
                 const uint64_t hzN1 = (hzN >> 8) |
                                       (uint64_t((NR & side_sel(0, 0, -1)) && ((N >> 56) & side_sel(0, 0, 1))) << 56);
-                c[0] &= ~(c[1] & hzN);
-                c[2] &= ~(c[1] & hzN1);
+                c[0] &= ~(raw1 & hzN);
+                c[2] &= ~(raw1 & hzN1);
                 uint64_t todo = c[0] | c[1] | c[2];
                 while (todo) {
                     const int k = (__ffsll(todo) - 1) >> 3;
@@ -440,9 +443,27 @@ __device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
 
 }  // namespace
 
+// Per-CTA set of node pairs already unioned for the current tile (open addressing on 64-bit
+// keys); dense volumes produce the same pair from hundreds of face blocks.
+constexpr int kPairSlots = 2048;
+
+__device__ __forceinline__ bool pair_first_seen(unsigned long long *set, uint32_t a, uint32_t b)
+{
+    const unsigned long long key = (uint64_t(a) << 32) | b;
+    uint32_t h = (a * 0x9E3779B1u) ^ (b * 0x85EBCA77u);
+    for (int probe = 0; probe < 8; ++probe) {
+        const uint32_t i = (h + probe) & (kPairSlots - 1);
+        const unsigned long long old = atomicCAS(&set[i], ~0ull, key);
+        if (old == ~0ull) return true;   // inserted: first occurrence
+        if (old == key) return false;    // already done by another thread
+    }
+    return true;                         // table crowded: just do the union
+}
+
 __global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work w)
 {
     __shared__ uint32_t qslot;
+    __shared__ unsigned long long pairs[kPairSlots];
     constexpr int NPLUS = TB1 * TB2 + TB0 * TB2 + TB0 * TB1;
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
@@ -452,6 +473,8 @@ __global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work 
         const int tb[3] = {TB0, TB1, TB2};
         const int tc[3] = {g.tx0, g.tx1, g.tx2};
         const int tn[3] = {im.t0, im.t1, im.t2};
+        for (int i = threadIdx.x; i < kPairSlots; i += kT3MergeThreads) pairs[i] = ~0ull;
+        __syncthreads();
         for (int p = threadIdx.x; p < NPLUS; p += kT3MergeThreads) {
             int axis, q;
             if (p < TB1 * TB2) { axis = 0; q = p; }
@@ -494,10 +517,11 @@ __global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work 
                     for (int q2 = 0; q2 < ndone; ++q2) seen |= done[q2] == nB;
                     if (seen) continue;
                     done[ndone++] = nB;
-                    gunion3d(im, w, nA, nB);
+                    if (pair_first_seen(pairs, nA, nB)) gunion3d(im, w, nA, nB);
                 }
             }
         }
+        __syncthreads();
     }
 }
 
