@@ -38,7 +38,8 @@ typedef enum be_status {
     BE_ERR_CUDA = 4,           /* a CUDA call failed; see be_last_error */
     BE_ERR_TIMEOUT = 5,        /* a bounded wait ran out (server / batch) */
     BE_ERR_BUSY = 6,           /* admission refused: not enough free device memory or slots */
-    BE_ERR_CANCELLED = 7       /* the request was cancelled before it completed */
+    BE_ERR_CANCELLED = 7,      /* the request was cancelled before it completed */
+    BE_ERR_TOO_LARGE = 8       /* the image exceeds the fixed scratch of be_label2d_noalloc */
 } be_status;
 
 /* Merge algorithm. */
@@ -93,6 +94,20 @@ int be_label2d_host(be_ctx *ctx, const uint8_t *in, int64_t in_pitch, int32_t ro
 int be_label3d_host(be_ctx *ctx, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
                     int threshold, int algo, int32_t *out, int64_t *n_components,
                     double *elapsed_us);
+
+/* 2D labeling that allocates no memory (no counterpart in the reference).  For callers that
+ * cannot call cudaMalloc -- a framework that already owns the device memory pool, a latency-bound
+ * loop that must not stall on cudaMalloc's implicit synchronization, a plugin host that forbids
+ * allocation.  Same computation and result as be_label2d (8-connectivity, union-find form), but the
+ * scratch is one fixed array inside the library's device image, held by every GPU that loads the
+ * library until exit.  Limit: at most 1024 tiles of 64 x 256 pixels and rows x ceil(cols / 256) <=
+ * 65536 (4096 x 4096 fits); larger images return BE_ERR_TOO_LARGE.  The first call on a device
+ * looks the array's device address up (cudaGetSymbolAddress) with that device current; make it
+ * before any stream capture.  All calls share the array: calls whose work overlaps on the GPU
+ * race, so order them (one stream, or events).  n_components, if not NULL, receives K after a
+ * synchronization of `stream`.  No context, so no be_last_error message: the status says it all. */
+int be_label2d_noalloc(const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols, int threshold,
+                       int32_t *out, int64_t out_pitch, int64_t *n_components, void *stream);
 
 /* Report of the bounds-checked debug build (-DBE_BOUNDS_CHECK; no counterpart in the
  * reference): out3 = {site, value low, value high} of the first failed index check of the last

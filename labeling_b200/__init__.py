@@ -28,7 +28,8 @@ LIB_PATH = os.environ.get("BE_B200_LIB") or os.path.join(_HERE, "libbe_b200.so")
 
 BE_OK = 0
 STATUS = {0: "BE_OK", 1: "BE_ERR_INVALID", 2: "BE_ERR_OOM", 3: "BE_ERR_NO_CONVERGENCE",
-          4: "BE_ERR_CUDA", 5: "BE_ERR_TIMEOUT", 6: "BE_ERR_BUSY", 7: "BE_ERR_CANCELLED"}
+          4: "BE_ERR_CUDA", 5: "BE_ERR_TIMEOUT", 6: "BE_ERR_BUSY", 7: "BE_ERR_CANCELLED",
+          8: "BE_ERR_TOO_LARGE"}
 ALGO_AUTO, ALGO_UF, ALGO_ITER = 0, 1, 2
 COH_4, COH_8, COH_DEFAULT = 0, 1, 2
 
