@@ -317,6 +317,106 @@ def bench_ours(args, rank, world, local_rank):
     return result
 
 
+def bench_batch(args, rank, world, local_rank):
+    """4096 2D images, sides log-uniform in [64, 2048], Bernoulli density U[0.2, 0.8]: one batched
+    CUDA-graph launch (autotuned) against 4096 plain per-image calls, both on one stream."""
+    import ctypes
+    import torch
+    import labeling_b200 as be
+    from labeling_b200 import workloads as W
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.batch_images
+    sides = W.log_uniform_sides(n, 64, 2048, seed=1000 + rank)
+    rng = np.random.default_rng(2000 + rank)
+    dens = rng.uniform(0.2, 0.8, n)
+    g = torch.Generator(device=dev).manual_seed(3000 + rank)
+    d_in, d_out = [], []
+    for (h, w), p in zip(sides, dens):
+        d_in.append(((torch.rand((h, w), generator=g, device=dev) < float(p)).to(torch.uint8) * 255))
+        d_out.append(torch.empty((h, w), dtype=torch.int32, device=dev))
+    npx = sum(h * w for h, w in sides)
+    ctx = be.Context(local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(stream):
+        batch = be.Batch(ctx, list(zip(d_in, d_out)))
+        choice = batch.tune(stream)
+        for _ in range(max(args.warmup, 3)):
+            batch.run(stream)
+        stream.synchronize()
+        counts = batch.counts(stream)
+        if world > 1:
+            torch.distributed.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        with ClockSampler(local_rank) as clk:
+            for a, b in ev:
+                a.record(stream)
+                batch.run(stream)
+                b.record(stream)
+            torch.cuda.synchronize()
+        t_ms = sum(a.elapsed_time(b) for a, b in ev)
+        # 4096 plain per-image calls (the C entry point called directly, no count read-back)
+        f = be.lib().be_label2d
+        sp = stream.cuda_stream
+        args_list = [(ctx.handle, x.data_ptr(), int(x.stride(0)), int(x.shape[0]), int(x.shape[1]), 0,
+                      be.COH_DEFAULT, be.ALGO_UF, y.data_ptr(), int(y.stride(0)), None, sp)
+                     for x, y in zip(d_in, d_out)]
+        for a_ in args_list[:64]:
+            f(*a_)
+        stream.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for a_ in args_list:
+            f(*a_)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = p0.elapsed_time(p1)
+    if world > 1:
+        tt = torch.tensor([t_ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * npx * args.steps / (t_ms / 1e3) / 1e9
+    plain = npx / (plain_ms / 1e3) / 1e9
+    # end to end: pinned host images -> device -> batch graph -> labels back to pinned host
+    h_in = [x.cpu().pin_memory() for x in d_in]
+    h_out = [torch.empty(x.shape, dtype=torch.int32).pin_memory() for x in d_in]
+    e2e_steps = 2
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for _ in range(e2e_steps):
+            for hi, di in zip(h_in, d_in):
+                di.copy_(hi, non_blocking=True)
+            batch.run(stream)
+            for ho, do in zip(h_out, d_out):
+                ho.copy_(do, non_blocking=True)
+            stream.synchronize()
+    e2e_s = time.perf_counter() - t0
+    peak, peak_kind = load_peaks()
+    achieved = 5.0 * npx / (t_ms / args.steps / 1e3) / 1e9
+    batch.close()
+    ctx.close()
+    return {
+        "metric": "Gpx/s labeled (batched 2D BE, 4096 uneven images, one CUDA graph)",
+        "value": round(value, 3), "unit": "Gpx/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(t_ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "batch", "images": n, "side": "log-uniform [64, 2048]",
+                   "density": "U[0.2, 0.8]", "pixels": npx, "l2": "inputs 1.3 GB > L2",
+                   "tuned_choice": choice, "parallelism": f"replicas x{world}"},
+        "plain_per_image": {"value": round(plain, 3), "unit": "Gpx/s", "ms": round(plain_ms, 3)},
+        "batched_vs_plain": round(value / world / plain, 2),
+        "e2e": {"value": round(npx * e2e_steps / e2e_s / 1e9, 3), "unit": "Gpx/s",
+                "h2d_bytes_per_step": int(npx), "d2h_bytes_per_step": int(4 * npx)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                     "scope": "whole batch (one graph), 5 B/px"},
+        "gpu_launches": 5 * args.steps, "clocks": clk.summary(),
+        "components_total": int(sum(counts)),
+    }
+
+
 def bench_reference(args, rank, world):
     if rank != 0:
         return None
@@ -345,8 +445,9 @@ def main():
     ap.add_argument("--steps", type=int, default=28)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="2d8192", choices=["2d8192", "2d2048", "3d512"])
+    ap.add_argument("--workload", default="2d8192", choices=["2d8192", "2d2048", "3d512", "batch"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--batch-images", type=int, default=4096)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -362,7 +463,8 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    res = bench_ours(args, rank, world, local_rank)
+    res = bench_batch(args, rank, world, local_rank) if args.workload == "batch" else \
+        bench_ours(args, rank, world, local_rank)
     if world > 1:
         import torch
         torch.distributed.barrier()

@@ -95,6 +95,48 @@ int be_label3d_host(be_ctx *ctx, const uint8_t *in, int32_t d0, int32_t d1, int3
                     int threshold, int algo, int32_t *out, int64_t *n_components,
                     double *elapsed_us);
 
+/* ---- Autotuner (no counterpart in the reference) ----------------------------------------------
+ * Times the candidate forms -- the union-find pipeline in each 2D tile shape (32x128, 64x64,
+ * 16x256 blocks) and the iterative scan/analyze form -- on the caller's own input, checks that all
+ * of them give identical labels, and remembers the fastest for the input's size class; later
+ * BE_ALGO_AUTO calls of that class use it.  `out` receives the labels.  choice: 0..2 = tile
+ * shape of the union-find form, 16 = iterative form. */
+int be_autotune2d(be_ctx *ctx, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols,
+                  int threshold, int32_t *out, int64_t out_pitch, int *choice, void *stream);
+int be_autotune3d(be_ctx *ctx, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int threshold,
+                  int32_t *out, int *choice, void *stream);
+/* Tuning table to / from a text file ("class algo shape microseconds" per line). */
+int be_tune_save(const be_ctx *ctx, const char *path);
+int be_tune_load(be_ctx *ctx, const char *path);
+
+/* ---- Batched labeling (no counterpart in the reference, which loops over files on the host,
+ * main.cpp:309-340) ------------------------------------------------------------------------------
+ * One batch = any mix of 2D images and 3D volumes of any sizes, labeled by ONE launch sequence
+ * captured in a CUDA graph: persistent CTAs pull tiles of all images from atomic work queues.
+ * Buffers stay owned by the caller and must stay valid while the batch exists (the graph holds
+ * their addresses). */
+typedef struct be_image {
+    const uint8_t *in;   /* 2D: rows x cols, in_pitch bytes per row; 3D: dense [d0][d1][d2] */
+    int32_t *out;        /* int32 labels, same layout (2D: out_pitch elements per row) */
+    int64_t in_pitch;
+    int64_t out_pitch;
+    int32_t dims[3];     /* 2D: {rows, cols, 0}; 3D: {d0, d1, d2} */
+    int32_t threshold;   /* foreground is pixel > threshold */
+} be_image;
+
+enum { BE_BATCH_ONE_CTA_PER_TILE = 0x100 /* no persistent CTAs / work queue */ };
+
+typedef struct be_batch be_batch;
+int be_batch_create(be_ctx *ctx, const be_image *imgs, int n, int flags, be_batch **batch);
+/* Launches the batch's graph on `stream` (asynchronous). */
+int be_batch_run(be_batch *batch, void *stream);
+/* Component count of every image, in the caller's order (synchronizes `stream`). */
+int be_batch_counts(be_batch *batch, int64_t *counts, void *stream);
+/* Times the 2D tile shapes and persistent vs one-CTA-per-tile launches on this batch and keeps
+ * the fastest graph; *choice = shape | flags. */
+int be_batch_tune(be_batch *batch, void *stream, int *choice);
+int be_batch_destroy(be_batch *batch);
+
 /* 2D labeling that allocates no memory (no counterpart in the reference).  For callers that
  * cannot call cudaMalloc -- a framework that already owns the device memory pool, a latency-bound
  * loop that must not stall on cudaMalloc's implicit synchronization, a plugin host that forbids

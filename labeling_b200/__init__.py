@@ -34,6 +34,14 @@ ALGO_AUTO, ALGO_UF, ALGO_ITER = 0, 1, 2
 COH_4, COH_8, COH_DEFAULT = 0, 1, 2
 
 _lib = None
+BATCH_ONE_CTA_PER_TILE = 0x100
+
+
+class BEImage(ctypes.Structure):
+    """``be_image`` of include/be.h: one image (dims = (rows, cols, 0)) or volume of a batch."""
+    _fields_ = [("in_", ctypes.c_void_p), ("out", ctypes.c_void_p), ("in_pitch", ctypes.c_int64),
+                ("out_pitch", ctypes.c_int64), ("dims", ctypes.c_int32 * 3),
+                ("threshold", ctypes.c_int32)]
 
 
 class BEError(RuntimeError):
@@ -62,6 +70,15 @@ def lib() -> ctypes.CDLL:
     l.be_label3d.argtypes = [vp, vp, i32, i32, i32, c_int, c_int, vp, p64, vp]
     l.be_label2d_host.argtypes = [vp, vp, i64, i32, i32, c_int, c_int, c_int, vp, i64, p64, pdbl]
     l.be_label3d_host.argtypes = [vp, vp, i32, i32, i32, c_int, c_int, vp, p64, pdbl]
+    l.be_autotune2d.argtypes = [vp, vp, i64, i32, i32, c_int, vp, i64, ctypes.POINTER(c_int), vp]
+    l.be_autotune3d.argtypes = [vp, vp, i32, i32, i32, c_int, vp, ctypes.POINTER(c_int), vp]
+    l.be_tune_save.argtypes = [vp, ctypes.c_char_p]
+    l.be_tune_load.argtypes = [vp, ctypes.c_char_p]
+    l.be_batch_create.argtypes = [vp, ctypes.POINTER(BEImage), c_int, c_int, ctypes.POINTER(vp)]
+    l.be_batch_run.argtypes = [vp, vp]
+    l.be_batch_counts.argtypes = [vp, p64, vp]
+    l.be_batch_tune.argtypes = [vp, vp, ctypes.POINTER(c_int)]
+    l.be_batch_destroy.argtypes = [vp]
     l.be_set_stage_timing.argtypes = [vp, c_int]
     l.be_check_status.argtypes = [vp, c_int, ctypes.POINTER(ctypes.c_uint32)]
     l.be_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), c_int, ctypes.POINTER(c_int)]
@@ -98,6 +115,12 @@ class Context:
         out = (ctypes.c_uint32 * 3)()
         self.check(lib().be_check_status(self.handle, dims, out))
         return int(out[0]), int(out[1]) | (int(out[2]) << 32)
+
+    def tune_save(self, path: str) -> None:
+        self.check(lib().be_tune_save(self.handle, path.encode()))
+
+    def tune_load(self, path: str) -> None:
+        self.check(lib().be_tune_load(self.handle, path.encode()))
 
     def set_stage_timing(self, on: bool) -> None:
         self.check(lib().be_set_stage_timing(self.handle, int(on)))
@@ -198,6 +221,73 @@ def label3d_host(ctx: Context, vol: np.ndarray, threshold: int = 0, algo: int = 
     ctx.check(lib().be_label3d_host(ctx.handle, vol.ctypes.data, *vol.shape, threshold, algo,
                                     out.ctypes.data, ctypes.byref(n), ctypes.byref(us)))
     return out, int(n.value), float(us.value)
+
+
+def autotune2d(ctx: Context, img, out, threshold: int = 0, stream=None) -> int:
+    """Times every 2D form on this device image, keeps the fastest for its size class; returns
+    the choice (0..2 = union-find tile shape, 16 = iterative form)."""
+    ch = ctypes.c_int(-1)
+    ctx.check(lib().be_autotune2d(ctx.handle, _ptr(img), int(img.stride(0)), int(img.shape[0]),
+                                  int(img.shape[1]), threshold, _ptr(out), int(out.stride(0)),
+                                  ctypes.byref(ch), _stream(stream)))
+    return ch.value
+
+
+def autotune3d(ctx: Context, vol, out, threshold: int = 0, stream=None) -> int:
+    ch = ctypes.c_int(-1)
+    ctx.check(lib().be_autotune3d(ctx.handle, _ptr(vol), *(int(x) for x in vol.shape), threshold,
+                                  _ptr(out), ctypes.byref(ch), _stream(stream)))
+    return ch.value
+
+
+class Batch:
+    """A fixed list of device images / volumes labeled by one CUDA-graph launch (be_batch_*).
+    ``items``: sequence of (in_tensor, out_tensor[, threshold]); 2D tensors are images, 3D tensors
+    dense volumes.  The tensors must outlive the batch."""
+
+    def __init__(self, ctx: Context, items, flags: int = 0):
+        self.ctx = ctx
+        arr = (BEImage * len(items))()
+        self._keep = []
+        for i, it in enumerate(items):
+            t_in, t_out = it[0], it[1]
+            thr = it[2] if len(it) > 2 else 0
+            e = arr[i]
+            e.in_, e.out, e.threshold = _ptr(t_in), _ptr(t_out), int(thr)
+            if t_in.dim() == 2:
+                e.dims[0], e.dims[1], e.dims[2] = int(t_in.shape[0]), int(t_in.shape[1]), 0
+                e.in_pitch, e.out_pitch = int(t_in.stride(0)), int(t_out.stride(0))
+            else:
+                e.dims[0], e.dims[1], e.dims[2] = (int(x) for x in t_in.shape)
+                e.in_pitch = e.out_pitch = 0
+            self._keep.append((t_in, t_out))
+        self.n = len(items)
+        self._h = ctypes.c_void_p()
+        ctx.check(lib().be_batch_create(ctx.handle, arr, len(items), flags, ctypes.byref(self._h)))
+
+    def run(self, stream=None) -> None:
+        self.ctx.check(lib().be_batch_run(self._h, _stream(stream)))
+
+    def counts(self, stream=None):
+        out = (ctypes.c_int64 * self.n)()
+        self.ctx.check(lib().be_batch_counts(self._h, out, _stream(stream)))
+        return [int(x) for x in out]
+
+    def tune(self, stream=None) -> int:
+        ch = ctypes.c_int(-1)
+        self.ctx.check(lib().be_batch_tune(self._h, _stream(stream), ctypes.byref(ch)))
+        return ch.value
+
+    def close(self) -> None:
+        if self._h:
+            lib().be_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # --- the reference's labeler interface (ILabeling / IOCLLabeling3D shape) --------------------

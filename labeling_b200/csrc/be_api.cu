@@ -37,15 +37,7 @@ int cuda_error(be_ctx *ctx, cudaError_t e, const char *what)
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-Geometry geometry_2d()
-{
-    Geometry g;
-    g.lab_bytes_per_tile = size_t(T2_TBW) * T2_TBH * sizeof(uint16_t);
-    g.rbits_bytes_per_tile = size_t(2 * T2_TBH) * (2 * T2_TBW / 32) * sizeof(uint32_t);
-    g.nperim = T2_NPERIM;
-    g.maxb = T2_MAXB;
-    return g;
-}
+Geometry geometry_2d() { return uf2d_geometry(0); }
 
 Geometry geometry_3d()
 {
@@ -95,38 +87,26 @@ size_t layout_work(const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_img
 
 int Workspace::ensure(be_ctx *ctx, const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_imgs)
 {
-    if (base && n_tiles <= cap_tiles && n_segs <= cap_segs && n_imgs <= cap_imgs) {
-        layout_work(g, cap_tiles, cap_segs, cap_imgs, static_cast<char *>(base), &w);
-        w.n_tiles = n_tiles;
-        w.n_segs = n_segs;
-        w.n_chunks = int32_t((n_segs + kScanChunk - 1) / kScanChunk);
-        w.n_imgs = n_imgs;
-        return BE_OK;
+    const size_t need = layout_work(g, n_tiles, n_segs, n_imgs, nullptr, nullptr);
+    if (!base || need > bytes) {
+        if (base) {
+            cudaError_t e = cudaFree(base);
+            base = nullptr;
+            bytes = 0;
+            if (e != cudaSuccess) return cuda_error(ctx, e, "cudaFree(workspace)");
+        }
+        const size_t grow = need + need / 4;   // headroom for slightly larger later calls
+        cudaError_t e = cudaMalloc(&base, grow);
+        if (e != cudaSuccess) {
+            base = nullptr;
+            return cuda_error(ctx, e, "cudaMalloc(workspace)");
+        }
+        bytes = grow;
     }
-    const int64_t nt = std::max(n_tiles, cap_tiles), ns = std::max(n_segs, cap_segs);
-    const int ni = std::max(n_imgs, cap_imgs);
-    const size_t need = layout_work(g, nt, ns, ni, nullptr, nullptr);
-    if (base) {
-        cudaError_t e = cudaFree(base);
-        base = nullptr;
-        cap_tiles = cap_segs = 0;
-        cap_imgs = 0;
-        if (e != cudaSuccess) return cuda_error(ctx, e, "cudaFree(workspace)");
-    }
-    cudaError_t e = cudaMalloc(&base, need);
-    if (e != cudaSuccess) {
-        base = nullptr;
-        return cuda_error(ctx, e, "cudaMalloc(workspace)");
-    }
-    bytes = need;
-    cap_tiles = nt;
-    cap_segs = ns;
-    cap_imgs = ni;
-    layout_work(g, nt, ns, ni, static_cast<char *>(base), &w);
-    w.n_tiles = n_tiles;
-    w.n_segs = n_segs;
-    w.n_chunks = int32_t((n_segs + kScanChunk - 1) / kScanChunk);
-    w.n_imgs = n_imgs;
+    layout_work(g, n_tiles, n_segs, n_imgs, static_cast<char *>(base), &w);
+    cap_tiles = n_tiles;
+    cap_segs = n_segs;
+    cap_imgs = n_imgs;
     return BE_OK;
 }
 
@@ -143,16 +123,18 @@ void Workspace::release()
 // Launch sequences.
 // ---------------------------------------------------------------------------------------------
 void fill_img2d(Img2D &im, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols, int thr,
-                int32_t *out, int64_t out_pitch, int64_t tile_base, int64_t seg_base, int index)
+                int32_t *out, int64_t out_pitch, int64_t tile_base, int64_t seg_base, int index,
+                int shape)
 {
+    const int tbw = kShapes2D[shape].tbw, tbh = kShapes2D[shape].tbh;
     im.in = in;
     im.out = out;
     im.in_pitch = in_pitch;
     im.out_pitch = out_pitch;
     im.rows = rows;
     im.cols = cols;
-    im.tiles_x = (cols + 2 * T2_TBW - 1) / (2 * T2_TBW);
-    im.tiles_y = (rows + 2 * T2_TBH - 1) / (2 * T2_TBH);
+    im.tiles_x = (cols + 2 * tbw - 1) / (2 * tbw);
+    im.tiles_y = (rows + 2 * tbh - 1) / (2 * tbh);
     im.tile_base = tile_base;
     im.seg_base = seg_base;
     im.thr = thr;
@@ -174,35 +156,6 @@ void fill_img3d(Img3D &im, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2
     im.seg_base = seg_base;
     im.thr = thr;
     im.index = index;
-}
-
-// Enqueues the five launches of the 2D union-find pipeline.  With persistent = true every kernel
-// runs grid = min(items, SMs x resident CTAs) CTAs that pull items from w.queue (which must be zero
-// at launch); otherwise one CTA per item.
-cudaError_t launch_uf2d(const ImgList2D &L, const Work &w, int sms, bool persistent, cudaStream_t s,
-                        cudaEvent_t *ev)
-{
-    auto mark = [&](int i) {
-        if (ev) cudaEventRecord(ev[i], s);
-    };
-    auto grid = [&](int64_t items, int per_sm) -> unsigned {
-        int64_t g = persistent ? std::min<int64_t>(items, int64_t(sms) * per_sm) : items;
-        return unsigned(std::max<int64_t>(g, 1));
-    };
-    Work wk = w;
-    if (!persistent) wk.queue = nullptr;
-    mark(0);
-    k_tile_local_2d<<<grid(w.n_tiles, 5), 256, 0, s>>>(L, wk);
-    mark(1);
-    k_merge_2d<<<grid(w.n_tiles, 8), T2_TBW + T2_TBH, 0, s>>>(L, wk);
-    mark(2);
-    k_post_2d<<<grid(w.n_tiles + w.n_chunks, 12), kPostThreads, 0, s>>>(L, wk);
-    mark(3);
-    k_segscan<<<unsigned(std::max(w.n_chunks, 1)), kScanThreads, 0, s>>>(wk);
-    mark(4);
-    k_tile_write_2d<<<grid(w.n_tiles, 6), 256, 0, s>>>(L, wk);
-    mark(5);
-    return cudaGetLastError();
 }
 
 cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persistent, cudaStream_t s,
@@ -344,21 +297,23 @@ int be_label2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_error(c, e, "cudaSetDevice");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int rc;
+    int rc, shape;
+    pick2d(c, rows, cols, algo, &algo, &shape);
+    c->last_algo = algo;
     if (algo == BE_ALGO_ITER) {
         rc = run_iter2d(c, in, in_pitch, rows, cols, threshold, out, out_pitch, s);
     } else {
         Img2D im;
-        fill_img2d(im, in, in_pitch, rows, cols, threshold, out, out_pitch, 0, 0, 0);
+        fill_img2d(im, in, in_pitch, rows, cols, threshold, out, out_pitch, 0, 0, 0, shape);
         const int64_t n_tiles = int64_t(im.tiles_x) * im.tiles_y;
         const int64_t n_segs = int64_t(rows) * im.tiles_x;
-        rc = c->ws2d.ensure(c, geometry_2d(), n_tiles, n_segs, 1);
+        rc = c->ws2d.ensure(c, uf2d_geometry(shape), n_tiles, n_segs, 1);
         if (rc) return rc;
         ImgList2D L{nullptr, 1, im};
 #ifdef BE_BOUNDS_CHECK
         cudaMemsetAsync(c->ws2d.w.err, 0, 16 * sizeof(uint32_t), s);
 #endif
-        e = launch_uf2d(L, c->ws2d.w, c->sms, false, s, c->timing ? c->stage_ev : nullptr);
+        e = uf2d_launch(shape, L, c->ws2d.w, c->sms, false, s, c->timing ? c->stage_ev : nullptr);
         c->timed_stages = c->timing ? kStages : 0;
         if (e != cudaSuccess) return cuda_error(c, e, "be_label2d launch");
     }
@@ -391,6 +346,8 @@ int be_label3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
     if (e != cudaSuccess) return cuda_error(c, e, "cudaSetDevice");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int rc;
+    pick3d(c, int64_t(d0) * d1 * d2, algo, &algo);
+    c->last_algo = algo;
     if (algo == BE_ALGO_ITER) {
         rc = run_iter3d(c, in, d0, d1, d2, threshold, out, s);
     } else {
@@ -469,11 +426,11 @@ int be_label2d_host(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows
     e = cudaMemcpy2DAsync(out, out_pitch * sizeof(int32_t), c->d_out, dpo * sizeof(int32_t),
                           cols * sizeof(int32_t), rows, cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_error(c, e, "download");
-    const int64_t *src = algo == BE_ALGO_ITER ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
+    const int64_t *src = c->last_algo == BE_ALGO_ITER ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
     e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(c, e, "be_label2d_host sync");
-    if (algo == BE_ALGO_ITER && c->iter_err && *c->iter_err)
+    if (c->last_algo == BE_ALGO_ITER && c->iter_err && *c->iter_err)
         return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label2d_host: iteration cap reached");
     n = c->h_ncomp[0];
     if (n_components) *n_components = n;
@@ -509,11 +466,11 @@ int be_label3d_host(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_
     cudaEventRecord(c->ev1, s);
     e = cudaMemcpyAsync(out, c->d_out, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_error(c, e, "download");
-    const int64_t *src = algo == BE_ALGO_ITER ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
+    const int64_t *src = c->last_algo == BE_ALGO_ITER ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
     e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(c, e, "be_label3d_host sync");
-    if (algo == BE_ALGO_ITER && c->iter_err && *c->iter_err)
+    if (c->last_algo == BE_ALGO_ITER && c->iter_err && *c->iter_err)
         return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label3d_host: iteration cap reached");
     if (n_components) *n_components = c->h_ncomp[0];
     if (elapsed_us) {

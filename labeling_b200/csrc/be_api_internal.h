@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 #include <string>
+#include <vector>
 
 namespace be {
 
@@ -18,7 +19,17 @@ struct Geometry {
     int maxb;
 };
 
-Geometry geometry_2d();
+// 2D tile shapes (in 2x2 blocks); shape 0 is the default.
+struct Shape2D {
+    int tbw, tbh;
+};
+constexpr int kNumShapes2D = 3;
+extern const Shape2D kShapes2D[kNumShapes2D];
+Geometry uf2d_geometry(int shape);
+cudaError_t uf2d_launch(int shape, const ImgList2D &L, const Work &w, int sms, bool persistent,
+                        cudaStream_t s, cudaEvent_t *ev = nullptr);
+
+Geometry geometry_2d();   // shape 0
 Geometry geometry_3d();
 size_t layout_work(const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_imgs, char *base, Work *w);
 
@@ -39,16 +50,25 @@ struct IterWork {
     size_t bytes = 0;
 };
 
+// One autotuner decision: size class -> algorithm (+ 2D tile shape), with the time it measured.
+struct TuneEntry {
+    uint32_t cls;
+    int algo;
+    int shape;
+    float us;
+};
+void pick2d(const struct ::be_ctx *c, int rows, int cols, int algo_in, int *algo, int *shape);
+void pick3d(const struct ::be_ctx *c, int64_t n, int algo_in, int *algo);
+
 int set_error(struct ::be_ctx *ctx, int code, const char *fmt, ...);
 int cuda_error(struct ::be_ctx *ctx, cudaError_t e, const char *what);
 
 void fill_img2d(Img2D &im, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols, int thr,
-                int32_t *out, int64_t out_pitch, int64_t tile_base, int64_t seg_base, int index);
+                int32_t *out, int64_t out_pitch, int64_t tile_base, int64_t seg_base, int index,
+                int shape = 0);
 void fill_img3d(Img3D &im, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int thr,
                 int32_t *out, int64_t tile_base, int64_t seg_base, int index);
 constexpr int kStages = 5;   // launches of one union-find pipeline
-cudaError_t launch_uf2d(const ImgList2D &L, const Work &w, int sms, bool persistent, cudaStream_t s,
-                        cudaEvent_t *ev = nullptr);
 cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persistent, cudaStream_t s,
                         cudaEvent_t *ev = nullptr);
 
@@ -75,4 +95,6 @@ struct be_ctx {
     bool timing = false;            // record an event between the launches of a plain call
     int timed_stages = 0;
     cudaEvent_t stage_ev[be::kStages + 1] = {};
+    std::vector<be::TuneEntry> tune;  // autotuner decisions
+    int last_algo = 1;                // algorithm the last label call actually ran
 };

@@ -437,10 +437,8 @@ int run_graph(be_ctx *c, G g, int64_t nblocks, int64_t nfinal, int64_t nwords, F
     if (e == cudaSuccess)
         e = chain(add_kernel(graph, &n, prev, it_count, nblk(nwords), NT, (const uint32_t *)g.rbits,
                              g.w.segcnt, nwords));
-    ImgList2D none{nullptr, 0, Img2D{}};
     if (e == cudaSuccess)
-        e = chain(add_kernel(graph, &n, prev, k_post_2d, unsigned(g.w.n_chunks), unsigned(kPostThreads),
-                             none, g.w));
+        e = chain(add_kernel(graph, &n, prev, k_chunk_sums, unsigned(g.w.n_chunks), unsigned(kPostThreads), g.w));
     if (e == cudaSuccess)
         e = chain(add_kernel(graph, &n, prev, k_segscan, unsigned(g.w.n_chunks), unsigned(kScanThreads), g.w));
     if (e == cudaSuccess) e = chain(add_kernel(graph, &n, prev, f_final, nblk(nfinal), NT, g));

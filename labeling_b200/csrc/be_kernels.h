@@ -3,7 +3,8 @@
 #pragma once
 #include "be_common.cuh"
 
-// 2D tile: 128 x 32 blocks = 256 x 64 pixels.
+// Default 2D tile (shape 0): 128 x 32 blocks = 256 x 64 pixels.  be_uf2d.cu also instantiates
+// 64 x 64 and 256 x 16 blocks (shapes 1 and 2).
 #define T2_TBW 128
 #define T2_TBH 32
 #define T2_NPERIM (2 * (T2_TBW + T2_TBH))
@@ -19,17 +20,13 @@
 
 namespace be {
 
-__global__ void k_tile_local_2d(ImgList2D L, Work w);
-__global__ void k_merge_2d(ImgList2D L, Work w);
-__global__ void k_post_2d(ImgList2D L, Work w);
-__global__ void k_tile_write_2d(ImgList2D L, Work w);
-
 __global__ void k_tile_local_3d(ImgList3D L, Work w);
 __global__ void k_merge_3d(ImgList3D L, Work w);
 __global__ void k_post_3d(ImgList3D L, Work w);
 __global__ void k_tile_write_3d(ImgList3D L, Work w);
 
 __global__ void k_segscan(Work w);
+__global__ void k_chunk_sums(Work w);
 
 constexpr int kPostThreads = 128;
 constexpr int kT3Threads = 256;

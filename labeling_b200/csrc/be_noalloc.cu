@@ -88,7 +88,7 @@ extern "C" int be_label2d_noalloc(const uint8_t *in, int64_t in_pitch, int32_t r
     w.n_imgs = 1;
     be::ImgList2D L{nullptr, 1, im};
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (be::launch_uf2d(L, w, 0, false, s) != cudaSuccess) return BE_ERR_CUDA;
+    if (be::uf2d_launch(0, L, w, 0, false, s) != cudaSuccess) return BE_ERR_CUDA;
     if (n_components) {
         if (cudaMemcpyAsync(n_components, w.ncomp, sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)

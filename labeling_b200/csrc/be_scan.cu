@@ -57,4 +57,11 @@ __global__ void __launch_bounds__(kScanThreads) k_segscan(Work w)
     if (c == gridDim.x - 1 && threadIdx.x == 0) w.segpref[w.n_segs] = off + ctot;
 }
 
+// Chunk sums alone (one CTA per chunk), for pipelines without border roots to rank.
+__global__ void __launch_bounds__(kPostThreads) k_chunk_sums(Work w)
+{
+    __shared__ uint32_t tmp[kPostThreads / 32 + 1];
+    chunk_sum<kPostThreads>(w, blockIdx.x, tmp);
+}
+
 }  // namespace be
