@@ -137,6 +137,56 @@ int be_batch_counts(be_batch *batch, int64_t *counts, void *stream);
 int be_batch_tune(be_batch *batch, void *stream, int *choice);
 int be_batch_destroy(be_batch *batch);
 
+/* ---- Serving loop (no counterpart in the reference) -----------------------------------------
+ * Continuous batching: requests submitted from any thread are admitted while their device memory
+ * fits the budget (default: 80% of free device memory at creation) and labeled in batches by the
+ * persistent-kernel pipeline; requests arriving while batches run join the next one; `lanes`
+ * batches can be in flight on separate streams.  Device buffers come from a memory pool that keeps
+ * its memory.  Results are the same as labeling each image alone. */
+enum { BE_REQ_DEVICE_BUFFERS = 1 /* in / out are device pointers: no copies */ };
+
+typedef struct be_request {
+    const uint8_t *in;   /* host (pinned for full overlap) or device, dense */
+    int32_t *out;        /* same kind as `in`, dense int32 labels */
+    int32_t dims[3];     /* 2D: {rows, cols, 0}; 3D: {d0, d1, d2} */
+    int32_t threshold;
+    int32_t flags;       /* BE_REQ_* */
+} be_request;
+
+typedef struct be_result {
+    int32_t status;      /* BE_OK, BE_ERR_OOM, BE_ERR_BUSY (can never fit), BE_ERR_CANCELLED, ... */
+    int64_t n_components;
+    double latency_us;   /* submit -> completion */
+} be_result;
+
+typedef struct be_server_config {
+    int32_t device;
+    int64_t max_device_bytes;          /* 0: 80% of the free memory at creation */
+    int32_t lanes;                     /* batches in flight at once (streams) */
+    int32_t max_batch;                 /* requests per batch */
+    int32_t inject_alloc_failure_every; /* tests: every n-th device allocation fails (0 = off) */
+} be_server_config;
+
+typedef struct be_serve_stats {
+    int64_t completed, rejected, failed, batches, pixels;
+    double p50_us, p99_us, mean_us, wall_s;
+    int64_t device_bytes_in_use, device_bytes_budget;
+} be_serve_stats;
+
+typedef struct be_server be_server;
+void be_server_default_config(be_server_config *cfg);
+int be_server_create(const be_server_config *cfg, be_server **server);
+int be_server_submit(be_server *server, const be_request *req, uint64_t *id);
+/* Waits for request `id` (timeout_us < 0: no limit; BE_ERR_TIMEOUT when it runs out) and returns
+ * its status; the request is forgotten afterwards. */
+int be_server_wait(be_server *server, uint64_t id, int64_t timeout_us, be_result *result);
+/* Queued requests are dropped; a running one completes on the GPU but is reported cancelled. */
+int be_server_cancel(be_server *server, uint64_t id);
+int be_server_stats(be_server *server, be_serve_stats *stats);
+int be_server_reset_stats(be_server *server);
+/* Drains every submitted request, then stops. */
+int be_server_destroy(be_server *server);
+
 /* 2D labeling that allocates no memory (no counterpart in the reference).  For callers that
  * cannot call cudaMalloc -- a framework that already owns the device memory pool, a latency-bound
  * loop that must not stall on cudaMalloc's implicit synchronization, a plugin host that forbids

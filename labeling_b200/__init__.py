@@ -44,6 +44,32 @@ class BEImage(ctypes.Structure):
                 ("threshold", ctypes.c_int32)]
 
 
+class BERequest(ctypes.Structure):
+    _fields_ = [("in_", ctypes.c_void_p), ("out", ctypes.c_void_p), ("dims", ctypes.c_int32 * 3),
+                ("threshold", ctypes.c_int32), ("flags", ctypes.c_int32)]
+
+
+class BEResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("n_components", ctypes.c_int64),
+                ("latency_us", ctypes.c_double)]
+
+
+class BEServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("max_device_bytes", ctypes.c_int64),
+                ("lanes", ctypes.c_int32), ("max_batch", ctypes.c_int32),
+                ("inject_alloc_failure_every", ctypes.c_int32)]
+
+
+class BEServeStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_int64), ("rejected", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("batches", ctypes.c_int64), ("pixels", ctypes.c_int64), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("wall_s", ctypes.c_double),
+                ("device_bytes_in_use", ctypes.c_int64), ("device_bytes_budget", ctypes.c_int64)]
+
+
+REQ_DEVICE_BUFFERS = 1
+
+
 class BEError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS.get(code, code)}: {msg}")
@@ -79,6 +105,14 @@ def lib() -> ctypes.CDLL:
     l.be_batch_counts.argtypes = [vp, p64, vp]
     l.be_batch_tune.argtypes = [vp, vp, ctypes.POINTER(c_int)]
     l.be_batch_destroy.argtypes = [vp]
+    l.be_server_default_config.argtypes = [ctypes.POINTER(BEServerConfig)]
+    l.be_server_create.argtypes = [ctypes.POINTER(BEServerConfig), ctypes.POINTER(vp)]
+    l.be_server_submit.argtypes = [vp, ctypes.POINTER(BERequest), ctypes.POINTER(ctypes.c_uint64)]
+    l.be_server_wait.argtypes = [vp, ctypes.c_uint64, i64, ctypes.POINTER(BEResult)]
+    l.be_server_cancel.argtypes = [vp, ctypes.c_uint64]
+    l.be_server_stats.argtypes = [vp, ctypes.POINTER(BEServeStats)]
+    l.be_server_reset_stats.argtypes = [vp]
+    l.be_server_destroy.argtypes = [vp]
     l.be_set_stage_timing.argtypes = [vp, c_int]
     l.be_check_status.argtypes = [vp, c_int, ctypes.POINTER(ctypes.c_uint32)]
     l.be_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), c_int, ctypes.POINTER(c_int)]
@@ -281,6 +315,69 @@ class Batch:
     def close(self) -> None:
         if self._h:
             lib().be_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching labeling server (be_server_*).  ``submit`` takes numpy arrays (host
+    requests; page-locked arrays give asynchronous copies) or CUDA tensors with device=True; the
+    arrays must stay alive until ``wait`` returns."""
+
+    def __init__(self, device: int = 0, lanes: int = 2, max_batch: int = 256,
+                 max_device_bytes: int = 0, inject_alloc_failure_every: int = 0):
+        cfg = BEServerConfig()
+        lib().be_server_default_config(ctypes.byref(cfg))
+        cfg.device, cfg.lanes, cfg.max_batch = device, lanes, max_batch
+        cfg.max_device_bytes, cfg.inject_alloc_failure_every = max_device_bytes, inject_alloc_failure_every
+        self._h = ctypes.c_void_p()
+        rc = lib().be_server_create(ctypes.byref(cfg), ctypes.byref(self._h))
+        if rc:
+            raise BEError(rc, "be_server_create failed")
+
+    def submit(self, img, out, threshold: int = 0, device: bool = False) -> int:
+        r = BERequest()
+        if device:
+            r.in_, r.out = _ptr(img), _ptr(out)
+        else:
+            assert img.flags.c_contiguous and out.flags.c_contiguous and out.dtype == np.int32
+            r.in_, r.out = img.ctypes.data, out.ctypes.data
+        shp = tuple(int(x) for x in img.shape)
+        r.dims[0], r.dims[1], r.dims[2] = shp[0], shp[1], shp[2] if len(shp) == 3 else 0
+        r.threshold, r.flags = threshold, REQ_DEVICE_BUFFERS if device else 0
+        i = ctypes.c_uint64(0)
+        rc = lib().be_server_submit(self._h, ctypes.byref(r), ctypes.byref(i))
+        if rc:
+            raise BEError(rc, "be_server_submit failed")
+        return int(i.value)
+
+    def wait(self, rid: int, timeout_us: int = -1):
+        """(status, n_components, latency_us); status BE_ERR_TIMEOUT leaves the request pending."""
+        res = BEResult()
+        st = lib().be_server_wait(self._h, rid, timeout_us, ctypes.byref(res))
+        if st == 5:
+            return 5, None, None
+        return int(res.status), int(res.n_components), float(res.latency_us)
+
+    def cancel(self, rid: int) -> int:
+        return lib().be_server_cancel(self._h, rid)
+
+    def stats(self) -> dict:
+        st = BEServeStats()
+        lib().be_server_stats(self._h, ctypes.byref(st))
+        return {f: getattr(st, f) for f, _ in BEServeStats._fields_}
+
+    def reset_stats(self) -> None:
+        lib().be_server_reset_stats(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            lib().be_server_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
