@@ -46,7 +46,10 @@ typedef enum be_status {
 enum {
     BE_ALGO_AUTO = 0, /* the autotuned choice (union-find unless the tuner measured otherwise) */
     BE_ALGO_UF = 1,   /* tile union-find in shared memory + global border merge */
-    BE_ALGO_ITER = 2  /* the paper's iterative scan / analyze, with a device-side change flag */
+    BE_ALGO_ITER = 2, /* the paper's iterative scan / analyze, with a device-side change flag */
+    BE_ALGO_PIXEL = 3 /* pixel-level label equivalence, the -a lbeq path (LabelingAlgs.cl:31-130,
+                         635-734): 2D 4-connectivity for BE_COH_4 / BE_COH_DEFAULT (the reference's
+                         default), 8 for BE_COH_8; 3D 26-connectivity */
 };
 
 /* Connectivity selector, as the reference's TCoherence (LabelingTools.hpp:45-50). */

@@ -30,7 +30,7 @@ BE_OK = 0
 STATUS = {0: "BE_OK", 1: "BE_ERR_INVALID", 2: "BE_ERR_OOM", 3: "BE_ERR_NO_CONVERGENCE",
           4: "BE_ERR_CUDA", 5: "BE_ERR_TIMEOUT", 6: "BE_ERR_BUSY", 7: "BE_ERR_CANCELLED",
           8: "BE_ERR_TOO_LARGE"}
-ALGO_AUTO, ALGO_UF, ALGO_ITER = 0, 1, 2
+ALGO_AUTO, ALGO_UF, ALGO_ITER, ALGO_PIXEL = 0, 1, 2, 3
 COH_4, COH_8, COH_DEFAULT = 0, 1, 2
 
 _lib = None
@@ -435,7 +435,7 @@ class Labeling3D:
 
 ALGORITHMS = {
     "bleq": ("Block equivalence by Zavalishin et.al. 2016", ALGO_AUTO),
-    "lbeq": ("Label equivalence (iterative scan/analyze form)", ALGO_ITER),
+    "lbeq": ("Label equivalence by Kalentev et.al. 2012 (pixel level)", ALGO_PIXEL),
 }
 
 

@@ -288,19 +288,21 @@ int be_label2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
         return set_error(c, BE_ERR_INVALID, "be_label2d: pitch smaller than the row");
     if (threshold < 0 || threshold > 255)
         return set_error(c, BE_ERR_INVALID, "be_label2d: threshold %d outside 0..255", threshold);
-    if (coh == BE_COH_4)
-        return set_error(c, BE_ERR_INVALID, "be_label2d: block equivalence does not support 4-connectivity");
-    if (coh != BE_COH_8 && coh != BE_COH_DEFAULT)
-        return set_error(c, BE_ERR_INVALID, "be_label2d: unknown connectivity %d", coh);
-    if (algo < BE_ALGO_AUTO || algo > BE_ALGO_ITER)
+    if (algo < BE_ALGO_AUTO || algo > BE_ALGO_PIXEL)
         return set_error(c, BE_ERR_INVALID, "be_label2d: unknown algorithm %d", algo);
+    if (coh == BE_COH_4 && algo != BE_ALGO_PIXEL)
+        return set_error(c, BE_ERR_INVALID, "be_label2d: block equivalence does not support 4-connectivity");
+    if (coh != BE_COH_4 && coh != BE_COH_8 && coh != BE_COH_DEFAULT)
+        return set_error(c, BE_ERR_INVALID, "be_label2d: unknown connectivity %d", coh);
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_error(c, e, "cudaSetDevice");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int rc, shape;
     pick2d(c, rows, cols, algo, &algo, &shape);
     c->last_algo = algo;
-    if (algo == BE_ALGO_ITER) {
+    if (algo == BE_ALGO_PIXEL) {
+        rc = run_lbeq2d(c, in, in_pitch, rows, cols, threshold, coh == BE_COH_8, out, out_pitch, s);
+    } else if (algo == BE_ALGO_ITER) {
         rc = run_iter2d(c, in, in_pitch, rows, cols, threshold, out, out_pitch, s);
     } else {
         Img2D im;
@@ -319,11 +321,11 @@ int be_label2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
     }
     if (rc) return rc;
     if (n_components) {
-        const int64_t *src = algo == BE_ALGO_ITER ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
+        const int64_t *src = (algo == BE_ALGO_ITER || algo == BE_ALGO_PIXEL) ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
         e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_error(c, e, "be_label2d sync");
-        if (algo == BE_ALGO_ITER && c->iter_err && *c->iter_err)
+        if ((algo == BE_ALGO_ITER || algo == BE_ALGO_PIXEL) && c->iter_err && *c->iter_err)
             return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label2d: iteration cap reached");
         *n_components = c->h_ncomp[0];
     }
@@ -340,7 +342,7 @@ int be_label3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
         return set_error(c, BE_ERR_INVALID, "be_label3d: bad size %d x %d x %d", d0, d1, d2);
     if (threshold < 0 || threshold > 255)
         return set_error(c, BE_ERR_INVALID, "be_label3d: threshold %d outside 0..255", threshold);
-    if (algo < BE_ALGO_AUTO || algo > BE_ALGO_ITER)
+    if (algo < BE_ALGO_AUTO || algo > BE_ALGO_PIXEL)
         return set_error(c, BE_ERR_INVALID, "be_label3d: unknown algorithm %d", algo);
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_error(c, e, "cudaSetDevice");
@@ -348,7 +350,9 @@ int be_label3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
     int rc;
     pick3d(c, int64_t(d0) * d1 * d2, algo, &algo);
     c->last_algo = algo;
-    if (algo == BE_ALGO_ITER) {
+    if (algo == BE_ALGO_PIXEL) {
+        rc = run_lbeq3d(c, in, d0, d1, d2, threshold, out, s);
+    } else if (algo == BE_ALGO_ITER) {
         rc = run_iter3d(c, in, d0, d1, d2, threshold, out, s);
     } else {
         Img3D im;
@@ -367,11 +371,11 @@ int be_label3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
     }
     if (rc) return rc;
     if (n_components) {
-        const int64_t *src = algo == BE_ALGO_ITER ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
+        const int64_t *src = (algo == BE_ALGO_ITER || algo == BE_ALGO_PIXEL) ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
         e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_error(c, e, "be_label3d sync");
-        if (algo == BE_ALGO_ITER && c->iter_err && *c->iter_err)
+        if ((algo == BE_ALGO_ITER || algo == BE_ALGO_PIXEL) && c->iter_err && *c->iter_err)
             return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label3d: iteration cap reached");
         *n_components = c->h_ncomp[0];
     }
@@ -426,11 +430,11 @@ int be_label2d_host(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows
     e = cudaMemcpy2DAsync(out, out_pitch * sizeof(int32_t), c->d_out, dpo * sizeof(int32_t),
                           cols * sizeof(int32_t), rows, cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_error(c, e, "download");
-    const int64_t *src = c->last_algo == BE_ALGO_ITER ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
+    const int64_t *src = (c->last_algo == BE_ALGO_ITER || c->last_algo == BE_ALGO_PIXEL) ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
     e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(c, e, "be_label2d_host sync");
-    if (c->last_algo == BE_ALGO_ITER && c->iter_err && *c->iter_err)
+    if ((c->last_algo == BE_ALGO_ITER || c->last_algo == BE_ALGO_PIXEL) && c->iter_err && *c->iter_err)
         return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label2d_host: iteration cap reached");
     n = c->h_ncomp[0];
     if (n_components) *n_components = n;
@@ -466,11 +470,11 @@ int be_label3d_host(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_
     cudaEventRecord(c->ev1, s);
     e = cudaMemcpyAsync(out, c->d_out, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_error(c, e, "download");
-    const int64_t *src = c->last_algo == BE_ALGO_ITER ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
+    const int64_t *src = (c->last_algo == BE_ALGO_ITER || c->last_algo == BE_ALGO_PIXEL) ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
     e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(c, e, "be_label3d_host sync");
-    if (c->last_algo == BE_ALGO_ITER && c->iter_err && *c->iter_err)
+    if ((c->last_algo == BE_ALGO_ITER || c->last_algo == BE_ALGO_PIXEL) && c->iter_err && *c->iter_err)
         return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label3d_host: iteration cap reached");
     if (n_components) *n_components = c->h_ncomp[0];
     if (elapsed_us) {

@@ -76,6 +76,10 @@ int run_iter2d(struct ::be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t 
                int thr, int32_t *out, int64_t out_pitch, cudaStream_t s);
 int run_iter3d(struct ::be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int thr,
                int32_t *out, cudaStream_t s);
+int run_lbeq2d(struct ::be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols, int thr,
+               int conn8, int32_t *out, int64_t out_pitch, cudaStream_t s);
+int run_lbeq3d(struct ::be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int thr,
+               int32_t *out, cudaStream_t s);
 
 }  // namespace be
 

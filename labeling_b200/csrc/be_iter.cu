@@ -331,6 +331,186 @@ __global__ void it_ncomp(Work w, const uint32_t *ctl, uint32_t *err_out)
     *err_out = ctl[2];
 }
 
+// ---- pixel-level label equivalence (-a lbeq -g) ------------------------------------------------
+// The reference's DistrInit/Scan/Analize (LabelingAlgs.cl:31-130) and LBEQ3D_* (:635-734):
+// every foreground pixel starts with its own label and the Scan / Analyze loop of the block form
+// runs on pixels.  2D: 4 neighbours (COH_4 and the reference's default) or 8 (COH_8); 3D: 26.
+// Labels are first-pixel keys as in the block form, so the output is canonical; the reference's
+// own quirk (a foreground pixel at (0, 0) keeps label 0, LabelingAlgs.cl:37, 48-50) is not
+// reproduced.
+struct Lq2 {
+    const uint8_t *in;
+    int64_t pitch;
+    int32_t *out;
+    int64_t opitch;
+    int rows, cols, sx, thr, conn8;
+    uint32_t *lab;
+    uint32_t *rbits;
+    uint32_t *ctl;
+    Work w;
+};
+
+struct Lq3 {
+    const uint8_t *in;
+    int32_t *out;
+    int d0, d1, d2, s1, s2, thr;
+    uint32_t *lab;
+    uint32_t *rbits;
+    uint32_t *ctl;
+    Work w;
+};
+
+__device__ __forceinline__ int64_t lq_pix2(const Lq2 &g, uint32_t key)
+{
+    return int64_t(key >> g.sx) * g.cols + (key & ((1u << g.sx) - 1u));
+}
+
+__global__ void __launch_bounds__(NT) lq_init_2d(Lq2 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.rows) * g.cols) return;
+    const int y = int(p / g.cols), x = int(p - int64_t(y) * g.cols);
+    g.lab[p] = g.in[int64_t(y) * g.pitch + x] > g.thr ? ((uint32_t(y) << g.sx) | uint32_t(x)) + 1u : 0u;
+}
+
+__global__ void __launch_bounds__(NT) lq_scan_2d(Lq2 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.rows) * g.cols) return;
+    const uint32_t label = g.lab[p];
+    if (!label) return;
+    const int y = int(p / g.cols), x = int(p - int64_t(y) * g.cols);
+    uint32_t m = 0xFFFFFFFFu;
+    for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+            if ((!dx && !dy) || (!g.conn8 && dx && dy)) continue;
+            const int ny = y + dy, nx = x + dx;
+            if (ny < 0 || nx < 0 || ny >= g.rows || nx >= g.cols) continue;
+            const uint32_t v = g.lab[int64_t(ny) * g.cols + nx];
+            if (v && v < m) m = v;
+        }
+    if (m < label) {
+        atomicMin(&g.lab[lq_pix2(g, label - 1)], m);
+        g.ctl[0] = 1;
+    }
+}
+
+__global__ void __launch_bounds__(NT) lq_analyze_2d(Lq2 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.rows) * g.cols) return;
+    uint32_t label = g.lab[p];
+    if (!label) return;
+    for (int step = 0;; ++step) {
+        const uint32_t nxt = g.lab[lq_pix2(g, label - 1)];
+        if (nxt == label) break;
+        if (step == kChaseCap) { g.ctl[2] = 1; break; }
+        label = nxt;
+    }
+    g.lab[p] = label;
+}
+
+__global__ void __launch_bounds__(NT) lq_mark_2d(Lq2 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.rows) * g.cols) return;
+    const uint32_t label = g.lab[p];
+    if (!label || lq_pix2(g, label - 1) != p) return;
+    const uint32_t k = label - 1;
+    atomicOr(&g.rbits[k >> 5], 1u << (k & 31));
+}
+
+__global__ void __launch_bounds__(NT) lq_final_2d(Lq2 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.rows) * g.cols) return;
+    const int y = int(p / g.cols), x = int(p - int64_t(y) * g.cols);
+    const uint32_t label = g.lab[p];
+    int32_t l = 0;
+    if (label) {
+        const uint32_t k = label - 1;
+        l = int32_t(1u + g.w.segpref[k >> 5] + __popc(g.rbits[k >> 5] & ((1u << (k & 31)) - 1u)));
+    }
+    g.out[int64_t(y) * g.opitch + x] = l;
+}
+
+__device__ __forceinline__ int64_t lq_pix3(const Lq3 &g, uint32_t key)
+{
+    const uint32_t Z = key & ((1u << g.s2) - 1u);
+    const uint32_t Y = (key >> g.s2) & ((1u << g.s1) - 1u);
+    const uint32_t X = key >> (g.s1 + g.s2);
+    return (int64_t(X) * g.d1 + Y) * g.d2 + Z;
+}
+
+__global__ void __launch_bounds__(NT) lq_init_3d(Lq3 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.d0) * g.d1 * g.d2) return;
+    const uint32_t Z = uint32_t(p % g.d2), Y = uint32_t((p / g.d2) % g.d1), X = uint32_t(p / (int64_t(g.d2) * g.d1));
+    g.lab[p] = g.in[p] > g.thr ? ((((X << g.s1) | Y) << g.s2) | Z) + 1u : 0u;
+}
+
+__global__ void __launch_bounds__(NT) lq_scan_3d(Lq3 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.d0) * g.d1 * g.d2) return;
+    const uint32_t label = g.lab[p];
+    if (!label) return;
+    const int Z = int(p % g.d2), Y = int((p / g.d2) % g.d1), X = int(p / (int64_t(g.d2) * g.d1));
+    uint32_t m = 0xFFFFFFFFu;
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz) {
+                if (!dx && !dy && !dz) continue;
+                const int nx = X + dx, ny = Y + dy, nz = Z + dz;
+                if (nx < 0 || ny < 0 || nz < 0 || nx >= g.d0 || ny >= g.d1 || nz >= g.d2) continue;
+                const uint32_t v = g.lab[(int64_t(nx) * g.d1 + ny) * g.d2 + nz];
+                if (v && v < m) m = v;
+            }
+    if (m < label) {
+        atomicMin(&g.lab[lq_pix3(g, label - 1)], m);
+        g.ctl[0] = 1;
+    }
+}
+
+__global__ void __launch_bounds__(NT) lq_analyze_3d(Lq3 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.d0) * g.d1 * g.d2) return;
+    uint32_t label = g.lab[p];
+    if (!label) return;
+    for (int step = 0;; ++step) {
+        const uint32_t nxt = g.lab[lq_pix3(g, label - 1)];
+        if (nxt == label) break;
+        if (step == kChaseCap) { g.ctl[2] = 1; break; }
+        label = nxt;
+    }
+    g.lab[p] = label;
+}
+
+__global__ void __launch_bounds__(NT) lq_mark_3d(Lq3 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.d0) * g.d1 * g.d2) return;
+    const uint32_t label = g.lab[p];
+    if (!label || lq_pix3(g, label - 1) != p) return;
+    const uint32_t k = label - 1;
+    atomicOr(&g.rbits[k >> 5], 1u << (k & 31));
+}
+
+__global__ void __launch_bounds__(NT) lq_final_3d(Lq3 g)
+{
+    const int64_t p = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (p >= int64_t(g.d0) * g.d1 * g.d2) return;
+    const uint32_t label = g.lab[p];
+    int32_t l = 0;
+    if (label) {
+        const uint32_t k = label - 1;
+        l = int32_t(1u + g.w.segpref[k >> 5] + __popc(g.rbits[k >> 5] & ((1u << (k & 31)) - 1u)));
+    }
+    g.out[p] = l;
+}
+
 unsigned nblk(int64_t n) { return unsigned((n + NT - 1) / NT); }
 
 int ceil_log2(int v)
@@ -415,7 +595,7 @@ int run_graph(be_ctx *c, G g, int64_t nblocks, int64_t nfinal, int64_t nwords, F
         e = chain(cudaGraphAddMemsetNode(&n, graph, &prev, 1, &m2));
     }
     if (e == cudaSuccess) e = chain(add_kernel(graph, &n, prev, f_init, nblk(nblocks), NT, g));
-    if (e == cudaSuccess) e = chain(add_kernel(graph, &n, prev, f_conn, nblk(nblocks), NT, g));
+    if (e == cudaSuccess && f_conn) e = chain(add_kernel(graph, &n, prev, f_conn, nblk(nblocks), NT, g));
     cudaGraphConditionalHandle h;
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
     if (e == cudaSuccess) {
@@ -513,6 +693,55 @@ int run_iter3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
     g.w.queue = nullptr;
     return run_graph(c, g, nblocks, int64_t(d0) * d1 * d2, nwords, it_init_3d, it_conn_3d, it_scan_3d,
                      it_analyze_3d, it_mark_3d, it_final_3d, s);
+}
+
+int run_lbeq2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols, int thr,
+               int conn8, int32_t *out, int64_t out_pitch, cudaStream_t s)
+{
+    Lq2 g{};
+    g.in = in; g.pitch = in_pitch; g.out = out; g.opitch = out_pitch;
+    g.rows = rows; g.cols = cols; g.thr = thr; g.conn8 = conn8;
+    g.sx = ceil_log2(cols);
+    const int64_t keyspace = int64_t(rows) << g.sx;
+    if (keyspace >= (int64_t(1) << 31))
+        return set_error(c, BE_ERR_INVALID, "label equivalence: %d x %d exceeds its key space", rows, cols);
+    const int64_t n = int64_t(rows) * cols, nwords = (keyspace + 31) / 32;
+    char *lab, *mk, *conn, *rb, *ctl;
+    int rc = iter_scratch(c, n, 0, nwords, &lab, &mk, &conn, &rb, &ctl);
+    if (rc) return rc;
+    rc = c->wsiter.ensure(c, geometry_2d(), 0, nwords, 1);
+    if (rc) return rc;
+    g.lab = reinterpret_cast<uint32_t *>(lab); g.rbits = reinterpret_cast<uint32_t *>(rb);
+    g.ctl = reinterpret_cast<uint32_t *>(ctl);
+    g.w = c->wsiter.w;
+    g.w.n_tiles = 0;
+    g.w.queue = nullptr;
+    return run_graph(c, g, n, n, nwords, lq_init_2d, (void (*)(Lq2)) nullptr, lq_scan_2d, lq_analyze_2d,
+                     lq_mark_2d, lq_final_2d, s);
+}
+
+int run_lbeq3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int thr, int32_t *out,
+               cudaStream_t s)
+{
+    Lq3 g{};
+    g.in = in; g.out = out; g.d0 = d0; g.d1 = d1; g.d2 = d2; g.thr = thr;
+    g.s1 = ceil_log2(d1); g.s2 = ceil_log2(d2);
+    const int64_t keyspace = int64_t(d0) << (g.s1 + g.s2);
+    if (keyspace >= (int64_t(1) << 31))
+        return set_error(c, BE_ERR_INVALID, "label equivalence: volume exceeds its key space");
+    const int64_t n = int64_t(d0) * d1 * d2, nwords = (keyspace + 31) / 32;
+    char *lab, *mk, *conn, *rb, *ctl;
+    int rc = iter_scratch(c, n, 0, nwords, &lab, &mk, &conn, &rb, &ctl);
+    if (rc) return rc;
+    rc = c->wsiter.ensure(c, geometry_2d(), 0, nwords, 1);
+    if (rc) return rc;
+    g.lab = reinterpret_cast<uint32_t *>(lab); g.rbits = reinterpret_cast<uint32_t *>(rb);
+    g.ctl = reinterpret_cast<uint32_t *>(ctl);
+    g.w = c->wsiter.w;
+    g.w.n_tiles = 0;
+    g.w.queue = nullptr;
+    return run_graph(c, g, n, n, nwords, lq_init_3d, (void (*)(Lq3)) nullptr, lq_scan_3d, lq_analyze_3d,
+                     lq_mark_3d, lq_final_3d, s);
 }
 
 }  // namespace be

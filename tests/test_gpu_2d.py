@@ -116,3 +116,29 @@ def test_large_image_repeated(ctx, p):
     for _ in range(3):
         lab, n = run2d(ctx, img)
         assert n == k and np.array_equal(lab, ref)
+
+
+@pytest.mark.parametrize("conn8", [False, True])
+def test_pixel_label_equivalence_lbeq(ctx, golden, conn8):
+    """-a lbeq -g: pixel-level label equivalence, 4-connectivity by default (the reference's
+    COH_DEFAULT) and 8 with -c 8.  Canonical labels equal the union-find oracle with the same
+    connectivity, and the reference's own lbeq labels (golden) after canonicalisation, except where
+    the reference's pixel-(0,0) quirk applies."""
+    import labeling_b200 as be
+    coh = be.COH_8 if conn8 else be.COH_DEFAULT
+    for (dim, name), c in golden.items():
+        if dim != "2d":
+            continue
+        img, thr = c["img"], int(c["thr"])
+        lab, n, _ = be.label2d_host(ctx, img, thr, be.ALGO_PIXEL, coh)
+        ref, k = O.ccl2d(img, thr, conn8=conn8)
+        assert n == k and np.array_equal(lab, ref), name
+        if img[0, 0] <= thr:
+            gold, _ = O.canon(c["distr8" if conn8 else "distr4"])
+            assert np.array_equal(lab, gold), name
+    from labeling_b200 import workloads as W
+    for p in (0.3, 0.55, 0.8):
+        img = W.bernoulli((700, 900), p, seed=int(100 * p))
+        lab, n, _ = be.label2d_host(ctx, img, 0, be.ALGO_PIXEL, coh)
+        ref, k = O.ccl2d(img, 0, conn8=conn8)
+        assert n == k and np.array_equal(lab, ref)

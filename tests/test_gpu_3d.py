@@ -83,3 +83,20 @@ def test_large_volume_repeated(ctx, p):
     for _ in range(3):
         lab, n = run3d(ctx, vol)
         assert n == k and np.array_equal(lab, ref)
+
+
+def test_pixel_label_equivalence_lbeq_3d(ctx, golden):
+    """-a lbeq -3 -g: voxel-level label equivalence, 26-connectivity; equals the reference's own
+    LBEQ3D labels (golden) after canonicalisation."""
+    import labeling_b200 as be
+    for (dim, name), c in golden.items():
+        if dim != "3d":
+            continue
+        lab, n, _ = be.label3d_host(ctx, c["img"], 0, be.ALGO_PIXEL)
+        gold, k = O.canon(c["lbeq"])
+        assert n == k and np.array_equal(lab, gold), name
+    from labeling_b200 import workloads as W
+    vol = W.bernoulli((70, 80, 90), 0.2, seed=12)
+    lab, n, _ = be.label3d_host(ctx, vol, 0, be.ALGO_PIXEL)
+    ref, k = O.ccl3d(vol)
+    assert n == k and np.array_equal(lab, ref)
