@@ -120,12 +120,14 @@ def make_2d_inputs(side: int, families, seed: int):
 
 
 def make_3d_inputs(side: int, seed: int):
+    import torch
     from labeling_b200 import workloads as W
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
     out = []
     for i, p in enumerate([0.1, 0.3, 0.5]):
         out.append((f"bern{p}", W.bernoulli((side, side, side), p, seed + i)))
     for pct in (50, 80):
-        out.append((f"grf{pct}", W.grf((side, side, side), 4.0, pct, seed + pct, device="cuda")))
+        out.append((f"grf{pct}", W.grf((side, side, side), 4.0, pct, seed + pct, device=dev)))
     return out
 
 
@@ -135,15 +137,21 @@ def make_3d_inputs(side: int, seed: int):
 
 def cpu_reference_2d(images, budget_s: float):
     """Times the reference's CPU labeler on whole images until budget_s is spent.  Prefers the
-    reference's OpenMP block-equivalence labeler (bleq CPU) and falls back to its Grana labeler."""
+    reference's OpenMP block-equivalence labeler (the bleq CPU slot, all host threads) timed by
+    its own stopwatch around DoLabel, and falls back to its single-threaded Grana labeler timed
+    around the call."""
     from oracle import oracle as O
-    kind_name = None
-    fn = None
-    if hasattr(O, "ref_cpu_bleq") and O.cpu_lib() is not None:
-        fn, kind_name = O.ref_cpu_bleq, "reference bleq CPU (TLabelEquivalenceX2, OpenMP)"
-        cores = os.cpu_count() or 1
+    if O.cpu_lib() is not None:
+        def fn(im):
+            return O.ref_cpu_bleq(im)[1] * 1e-6
+        kind_name = "reference bleq CPU (TLabelEquivalenceX2, OpenMP), own stopwatch"
+        cores = int(O.cpu_lib().ref_cpu_max_threads())
     elif O.grana_lib() is not None:
-        fn, kind_name = (lambda im: O.ref_grana(im)), "reference gr-block CPU (Grana, 1 thread)"
+        def fn(im):
+            t0 = time.perf_counter()
+            O.ref_grana(im)
+            return time.perf_counter() - t0
+        kind_name = "reference gr-block CPU (Grana, 1 thread)"
         cores = 1
     else:
         return None
@@ -152,9 +160,7 @@ def cpu_reference_2d(images, budget_s: float):
     i = 0
     while True:
         name, img = images[i % len(images)]
-        t0 = time.perf_counter()
-        fn(img)
-        t_total += time.perf_counter() - t0
+        t_total += fn(img)
         px += img.size
         n += 1
         i += 1
@@ -164,6 +170,32 @@ def cpu_reference_2d(images, budget_s: float):
             break
     return {"value": px / t_total / 1e9, "unit": "Gpx/s", "cores": cores,
             "kind": "reference", "sample": f"{n} whole images ({kind_name}), {t_total:.2f} s"}
+
+
+def cpu_reference_3d(volumes, budget_s: float):
+    """Times the reference's 3D block-equivalence path (its TOCLBlockEquivalence3D kernels,
+    LabelingAlgs.cl, compiled as C++ and run over all host threads; the reference has no CPU 3D
+    labeler of its own) on whole volumes until budget_s is spent, by the span of its kernel
+    sequence."""
+    from oracle import oracle as O
+    lib = O.ref_lib()
+    if lib is None:
+        return None
+    cores = int(lib.ref_set_threads(0))
+    lib.ref_set_threads(1)
+    px, t_total, n = 0, 0.0, 0
+    t_start = time.perf_counter()
+    i = 0
+    while True:
+        name, vol = volumes[i % len(volumes)]
+        t_total += O.ref_be3d_timed(vol, 0, 0)[1] * 1e-6
+        px += vol.size
+        n += 1
+        i += 1
+        if time.perf_counter() - t_start > budget_s or n >= len(volumes):
+            break
+    return {"value": px / t_total / 1e9, "unit": "Gvox/s", "cores": cores, "kind": "reference",
+            "sample": f"{n} whole volumes (reference bleq -3 kernels on the host, OpenMP), {t_total:.2f} s"}
 
 
 # ------------------------------------------------------------------------------------------
@@ -310,7 +342,7 @@ def bench_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         budget = 20.0
         if is3d:
-            result["cpu_baseline"] = None
+            result["cpu_baseline"] = cpu_reference_3d(inputs, budget)
         else:
             result["cpu_baseline"] = cpu_reference_2d(inputs, budget)
     ctx.close()
@@ -484,24 +516,30 @@ def bench_serve(args, rank, world, local_rank):
 
 
 def bench_reference(args, rank, world):
+    """The reference's own CPU implementation of the path on the host cores, bounded samples of
+    the same workload (rank 0 only)."""
     if rank != 0:
         return None
-    if args.workload == "3d512":
-        return {"impl": "reference", "unavailable": "the reference has no CPU 3D labeler (main.cpp:106,120,125)"}
-    side = 2048 if args.workload == "2d2048" else 8192
-    from labeling_b200 import workloads as W
-    fams = ["bern0.5"] if side == 2048 else W.FAMILIES_8192
-    inputs = make_2d_inputs(side, fams, seed=10)
-    for _ in range(max(0, min(args.warmup, 1))):
-        pass
-    cb = cpu_reference_2d(inputs, budget_s=30.0)
+    is3d = args.workload == "3d512"
+    if is3d:
+        inputs = make_3d_inputs(512, seed=100)
+        cb = cpu_reference_3d(inputs, budget_s=40.0)
+        metric, unit = "Gvox/s labeled (3D 512^3 BE, 26-conn)", "Gvox/s"
+        names = [n for n, _ in inputs]
+    else:
+        side = 2048 if args.workload == "2d2048" else 8192
+        from labeling_b200 import workloads as W
+        names = ["bern0.5"] if side == 2048 else W.FAMILIES_8192
+        inputs = make_2d_inputs(side, names, seed=10)
+        cb = cpu_reference_2d(inputs, budget_s=30.0)
+        metric, unit = f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "Gpx/s"
     if cb is None:
         return {"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}
-    return {"impl": "reference", "metric": f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "value": round(cb["value"], 4),
-            "unit": "Gpx/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+    return {"impl": "reference", "metric": metric, "value": round(cb["value"], 4),
+            "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-            "data": "synthetic (seeded)", "config": {"workload": args.workload, "images": fams},
-            "cpu_baseline": cb, "e2e": {"value": round(cb["value"], 4), "unit": "Gpx/s",
+            "data": "synthetic (seeded)", "config": {"workload": args.workload, "images": names},
+            "cpu_baseline": cb, "e2e": {"value": round(cb["value"], 4), "unit": unit,
                                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

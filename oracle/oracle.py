@@ -61,6 +61,10 @@ def ref_lib() -> Optional[ctypes.CDLL]:
         l.ref_bleq3d_raw.argtypes = [_u8p, _long, _long, _long, ctypes.c_int, _u32p]
         l.ref_distr2d_raw.argtypes = [_u8p, _long, _long, _long, ctypes.c_int, ctypes.c_int, _u32p]
         l.ref_lbeq3d_raw.argtypes = [_u8p, _long, _long, _long, ctypes.c_int, _u32p]
+        l.ref_bleq3d_timed.argtypes = [_u8p, _long, _long, _long, ctypes.c_int, _u32p,
+                                       ctypes.POINTER(ctypes.c_double)]
+        l.ref_set_threads.argtypes = [ctypes.c_int]
+        l.ref_set_threads.restype = ctypes.c_int
     return l
 
 
@@ -69,6 +73,16 @@ def grana_lib() -> Optional[ctypes.CDLL]:
     if l is not None:
         l.ref_grana.argtypes = [_u8p, _long, _long, _long, ctypes.c_int, _i32p,
                                 ctypes.POINTER(ctypes.c_int)]
+    return l
+
+
+def cpu_lib() -> Optional[ctypes.CDLL]:
+    """The reference's OpenMP CPU labelers (LabelingAlgs.cpp), compiled by `make -C oracle ref`."""
+    l = _load(os.path.join("_ref", "libref_cpu.so"))
+    if l is not None:
+        l.ref_cpu_label2d.argtypes = [ctypes.c_char_p, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, _i32p, ctypes.POINTER(ctypes.c_double)]
+        l.ref_cpu_max_threads.restype = ctypes.c_int
     return l
 
 
@@ -183,6 +197,25 @@ def ref_be3d_raw(vol: np.ndarray, thr: int = 0) -> np.ndarray:
     return out
 
 
+def ref_be3d_timed(vol: np.ndarray, thr: int = 0, threads: int = 1) -> Tuple[np.ndarray, float]:
+    """The reference's 3D block-equivalence kernels (TOCLBlockEquivalence3D) run on the host with
+    `threads` work-item threads (0 = all); returns the raw labels and the time of the kernel
+    sequence in microseconds."""
+    l = ref_lib()
+    if l is None:
+        raise RuntimeError("oracle/_ref/libref_be.so is not built")
+    vol = _u8(vol)
+    out = np.empty(vol.shape, np.uint32)
+    us = ctypes.c_double(0.0)
+    l.ref_set_threads(threads)
+    try:
+        if l.ref_bleq3d_timed(_p(vol, _u8p), *vol.shape, thr, _p(out, _u32p), ctypes.byref(us)):
+            raise RuntimeError("ref_bleq3d_timed failed")
+    finally:
+        l.ref_set_threads(1)
+    return out, float(us.value)
+
+
 def ref_distr2d_raw(img: np.ndarray, thr: int = 0, coh: int = 2) -> np.ndarray:
     l = ref_lib()
     if l is None:
@@ -204,6 +237,34 @@ def ref_lbeq3d_raw(vol: np.ndarray, thr: int = 0) -> np.ndarray:
     if l.ref_lbeq3d_raw(_p(vol, _u8p), *vol.shape, thr, _p(out, _u32p)):
         raise RuntimeError("ref_lbeq3d_raw failed")
     return out
+
+
+def ref_cpu_label2d(img: np.ndarray, alg: str = "bleq", thr: int = 0, threads: int = 0,
+                    coh: int = 1) -> Tuple[np.ndarray, float]:
+    """One of the reference's CPU labelers ("bleq" = TLabelEquivalenceX2, "lbeq" =
+    TLabelDistribution, "runeq" = TRunEqivLabeling, "gr-block" = Grana), run through
+    ILabeling::Label (LabelingTools.cpp:19-36) with `threads` OpenMP threads (0 = all).  Returns
+    the reference's raw labels and its own stopwatch time in microseconds.  The reference CPU
+    block labeler mis-connects blocks at an even-width right border (RemoveBorderBlocks compares
+    pixel coordinates with the image size, LabelingAlgs.cpp:366-374, so px == w - 1 never holds
+    and the x + 2 probes wrap into the next row), and TLabelDistribution leaves a foreground
+    pixel at (0, 0) unlabeled; both are the reference's behaviour, kept here as it is."""
+    l = cpu_lib()
+    if l is None:
+        raise RuntimeError("oracle/_ref/libref_cpu.so is not built")
+    img = _u8(img)
+    out = np.empty(img.shape, np.int32)
+    us = ctypes.c_double(0.0)
+    rc = l.ref_cpu_label2d(alg.encode(), _p(img, _u8p), img.shape[0], img.shape[1], thr, threads, coh,
+                           _p(out, _i32p), ctypes.byref(us))
+    if rc:
+        raise RuntimeError(f"ref_cpu_label2d({alg}) failed: {rc}")
+    return out, float(us.value)
+
+
+def ref_cpu_bleq(img: np.ndarray, thr: int = 0, threads: int = 0) -> Tuple[np.ndarray, float]:
+    """The reference's CPU block-equivalence labeler (the `bleq` CPU slot, main.cpp:122-126)."""
+    return ref_cpu_label2d(img, "bleq", thr, threads, 1)
 
 
 def ref_grana(img: np.ndarray, thr: int = 0) -> Tuple[np.ndarray, int]:

@@ -13,13 +13,17 @@
 namespace refcl {
 thread_local size_t gid[3];
 thread_local size_t gsz[3];
+int nthreads = 1;
 }  // namespace refcl
 
 #include REF_CL
 
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
+
+#include <omp.h>
 
 namespace {
 
@@ -71,7 +75,9 @@ int ref_lbeq2_raw(const uint8_t *img, long rows, long cols, long pitch, int thr,
 // TOCLBlockEquivalence3D::DoOCLLabel3D (LabelingAlgs.cpp:1520-1536) on the CopyAlignImg volume
 // (LabelingTools.cpp:160-176); the output is cropped back to d0 x d1 x d2 (the reference itself
 // returns the padded volume, LabelingTools.cpp:217-220).
-int ref_bleq3d_raw(const uint8_t *vol, long d0, long d1, long d2, int thr, uint32_t *out)
+// With usec, the time of the kernel sequence alone is written there (the span the reference's
+// stopwatch covers, LabelingTools.cpp:206-214).
+int ref_bleq3d_timed(const uint8_t *vol, long d0, long d1, long d2, int thr, uint32_t *out, double *usec)
 {
     if (d0 <= 0 || d1 <= 0 || d2 <= 0) return -1;
     const long X = ((d0 + 4) >> 5 << 5) + 32, Y = ((d1 + 4) >> 5 << 5) + 32,
@@ -86,6 +92,7 @@ int ref_bleq3d_raw(const uint8_t *vol, long d0, long d1, long d2, int thr, uint3
     const size_t sp[3] = {(size_t)X >> 1, (size_t)Y >> 1, (size_t)Z >> 1};
     std::vector<TLabel> sLabels(sp[0] * sp[1] * sp[2], 0);
     std::vector<int> sConn(sLabels.size(), 0);
+    const auto t0 = std::chrono::steady_clock::now();
     ref_ndrange(3, sp, [&] { BLEQ3D_Init(pix.data(), sLabels.data(), sConn.data()); });
     const size_t anSz[1] = {sLabels.size()};
     for (;;) {
@@ -96,11 +103,25 @@ int ref_bleq3d_raw(const uint8_t *vol, long d0, long d1, long d2, int thr, uint3
     }
     const size_t fin[3] = {(size_t)X, (size_t)Y, (size_t)Z};
     ref_ndrange(3, fin, [&] { BLEQ3D_SetFinalLabels(pix.data(), labels.data(), sLabels.data()); });
+    if (usec)
+        *usec = std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
     for (long x = 0; x < d0; ++x)
         for (long y = 0; y < d1; ++y)
             for (long z = 0; z < d2; ++z)
                 out[(x * d1 + y) * d2 + z] = labels[((size_t)(x + 2) * Y + (y + 2)) * Z + (z + 2)];
     return 0;
+}
+
+int ref_bleq3d_raw(const uint8_t *vol, long d0, long d1, long d2, int thr, uint32_t *out)
+{
+    return ref_bleq3d_timed(vol, d0, d1, d2, thr, out, nullptr);
+}
+
+// Work-item threads of every driver here: 1 = serial (the default), 0 = all OpenMP threads.
+int ref_set_threads(int n)
+{
+    refcl::nthreads = n > 0 ? n : omp_get_max_threads();
+    return refcl::nthreads;
 }
 
 // TOCLLabelDistribution::DoOCLLabel (LabelingAlgs.cpp:867-942): DistrInitKernel, then

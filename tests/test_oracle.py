@@ -83,3 +83,47 @@ def test_reference_quirks_are_reproduced(golden):
     c = golden[("2d", "checker_40")]
     k4 = len(np.unique(c["distr4"])) - 1
     assert k4 > 1 and int(c["k"]) == 1
+
+
+# --- the reference's own CPU code (oracle/_ref), present only where it was built ---------------
+
+needs_ref_cpu = pytest.mark.skipif(O.cpu_lib() is None, reason="oracle/_ref/libref_cpu.so not built")
+needs_ref_kernels = pytest.mark.skipif(O.ref_lib() is None, reason="oracle/_ref/libref_be.so not built")
+
+
+@needs_ref_cpu
+@pytest.mark.parametrize("seed", range(4))
+def test_reference_cpu_bleq_matches_oracle_inside_a_background_frame(seed):
+    """The reference's OpenMP block labeler (TLabelEquivalenceX2, the CPU baseline) gives the
+    oracle's partition once its border probes cannot wrap: a 2-pixel background frame."""
+    rng = np.random.default_rng(seed)
+    for _ in range(20):
+        h, w = rng.integers(1, 60, 2) * 2
+        img = np.zeros((h + 4, w + 4), np.uint8)
+        img[2:-2, 2:-2] = (rng.random((h, w)) < rng.uniform(0.2, 0.8)) * 255
+        raw, us = O.ref_cpu_bleq(img)
+        assert np.array_equal(O.canon(raw)[0], O.ccl2d(img)[0]) and us >= 0
+
+
+@needs_ref_cpu
+def test_reference_cpu_bleq_right_border_wrap_is_the_references():
+    """At the right border the reference's CPU block labeler reads the next row's first pixels
+    (RemoveBorderBlocks compares pixel coordinates with the image size, LabelingAlgs.cpp:366-374):
+    in this 4 x 2 image the two components come out as one.  The GPU path follows the reference's
+    GPU kernels, which pad the image and do not wrap."""
+    img = np.array([[1, 0], [0, 0], [1, 1], [1, 0]], np.uint8) * 255
+    raw, _ = O.ref_cpu_bleq(img)
+    assert O.canon(raw)[1] == 1 and O.ccl2d(img)[1] == 2
+
+
+@needs_ref_kernels
+def test_reference_3d_kernels_threaded_match_serial():
+    """The reference's 3D kernels on the host over OpenMP threads (the 3D CPU baseline) give the
+    serial sweep's partition and the oracle's."""
+    rng = np.random.default_rng(11)
+    for shape, p in [((21, 34, 47), 0.3), ((64, 64, 64), 0.25)]:
+        vol = ((rng.random(shape) < p) * 255).astype(np.uint8)
+        serial, _ = O.ref_be3d_timed(vol, 0, 1)
+        threaded, _ = O.ref_be3d_timed(vol, 0, 0)
+        ref = O.ccl3d(vol)[0]
+        assert np.array_equal(O.canon(serial)[0], ref) and np.array_equal(O.canon(threaded)[0], ref)
