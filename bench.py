@@ -119,15 +119,18 @@ def make_2d_inputs(side: int, families, seed: int):
     return [(f, W.family_8192(f, seed=seed + i, side=side)) for i, f in enumerate(families)]
 
 
-def make_3d_inputs(side: int, seed: int):
+def make_3d_inputs(side: int, seed: int, only: str = ""):
     import torch
     from labeling_b200 import workloads as W
     dev = "cuda" if torch.cuda.is_available() else "cpu"
+    keep = set(only.split(",")) if only else None
     out = []
     for i, p in enumerate([0.1, 0.3, 0.5]):
-        out.append((f"bern{p}", W.bernoulli((side, side, side), p, seed + i)))
+        if keep is None or f"bern{p}" in keep:
+            out.append((f"bern{p}", W.bernoulli((side, side, side), p, seed + i)))
     for pct in (50, 80):
-        out.append((f"grf{pct}", W.grf((side, side, side), 4.0, pct, seed + pct, device=dev)))
+        if keep is None or f"grf{pct}" in keep:
+            out.append((f"grf{pct}", W.grf((side, side, side), 4.0, pct, seed + pct, device=dev)))
     return out
 
 
@@ -135,41 +138,53 @@ def make_3d_inputs(side: int, seed: int):
 # Reference CPU labelers (oracle/_ref), bounded samples
 # ------------------------------------------------------------------------------------------
 
-def cpu_reference_2d(images, budget_s: float):
-    """Times the reference's CPU labeler on whole images until budget_s is spent.  Prefers the
-    reference's OpenMP block-equivalence labeler (the bleq CPU slot, all host threads) timed by
-    its own stopwatch around DoLabel, and falls back to its single-threaded Grana labeler timed
-    around the call."""
-    from oracle import oracle as O
-    if O.cpu_lib() is not None:
-        def fn(im):
-            return O.ref_cpu_bleq(im)[1] * 1e-6
-        kind_name = "reference bleq CPU (TLabelEquivalenceX2, OpenMP), own stopwatch"
-        cores = int(O.cpu_lib().ref_cpu_max_threads())
-    elif O.grana_lib() is not None:
-        def fn(im):
-            t0 = time.perf_counter()
-            O.ref_grana(im)
-            return time.perf_counter() - t0
-        kind_name = "reference gr-block CPU (Grana, 1 thread)"
-        cores = 1
-    else:
-        return None
+CPU_ALGS_2D = {
+    "bleq": "TLabelEquivalenceX2, block equivalence, OpenMP",
+    "runeq": "TRunEqivLabeling, run equivalence, OpenMP",
+    "gr-block": "TBlockGranaLabeling, Grana blocks, 1 thread",
+}
+
+
+def _time_cpu_alg(O, alg, images, budget_s):
     px, t_total, n = 0, 0.0, 0
     t_start = time.perf_counter()
-    i = 0
     while True:
-        name, img = images[i % len(images)]
-        t_total += fn(img)
+        name, img = images[n % len(images)]
+        t_total += O.ref_cpu_label2d(img, alg)[1] * 1e-6
         px += img.size
         n += 1
-        i += 1
-        if time.perf_counter() - t_start > budget_s and n >= min(len(images), 2):
+        if time.perf_counter() - t_start > budget_s or n >= 3 * len(images):
             break
-        if n >= 3 * len(images):
-            break
-    return {"value": px / t_total / 1e9, "unit": "Gpx/s", "cores": cores,
-            "kind": "reference", "sample": f"{n} whole images ({kind_name}), {t_total:.2f} s"}
+    return px / t_total / 1e9, n, t_total
+
+
+def cpu_reference_2d(images, budget_s: float):
+    """Times the reference's CPU labelers (its main.cpp registry's CPU slots, compiled from its
+    sources) on whole images, each by the reference's own stopwatch around DoLabel, all host
+    threads for the OpenMP ones.  The block-equivalence labeler (the bleq CPU slot) is the
+    reported baseline; run equivalence and Grana are listed beside it."""
+    from oracle import oracle as O
+    lib = O.cpu_lib()
+    if lib is None:
+        if O.grana_lib() is None:
+            return None
+        t0 = time.perf_counter()
+        n = min(len(images), 2)
+        for _, img in images[:n]:
+            O.ref_grana(img)
+        t = time.perf_counter() - t0
+        return {"value": sum(im.size for _, im in images[:n]) / t / 1e9, "unit": "Gpx/s", "cores": 1,
+                "kind": "reference", "sample": f"{n} whole images (gr-block, Grana, 1 thread), {t:.2f} s"}
+    cores = int(lib.ref_cpu_max_threads())
+    res = {}
+    for alg in CPU_ALGS_2D:
+        v, n, t = _time_cpu_alg(O, alg, images, budget_s / len(CPU_ALGS_2D))
+        res[alg] = {"value": round(v, 4), "cores": 1 if alg == "gr-block" else cores,
+                    "sample": f"{n} whole images, {t:.2f} s", "what": CPU_ALGS_2D[alg]}
+    main = res["bleq"]
+    return {"value": main["value"], "unit": "Gpx/s", "cores": cores, "kind": "reference",
+            "sample": f"bleq CPU slot ({CPU_ALGS_2D['bleq']}), {main['sample']}, reference stopwatch",
+            "others": {k: v for k, v in res.items() if k != "bleq"}}
 
 
 def cpu_reference_3d(volumes, budget_s: float):
@@ -210,12 +225,14 @@ def bench_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     is3d = args.workload == "3d512"
     if is3d:
-        inputs = make_3d_inputs(512, seed=100 + 17 * rank)
+        inputs = make_3d_inputs(512, seed=100 + 17 * rank, only=args.families)
         stages = STAGES_3D
         metric, unit = "Gvox/s labeled (3D 512^3 BE, 26-conn)", "Gvox/s"
     else:
         side = 2048 if args.workload == "2d2048" else 8192
         fams = ["bern0.5"] if side == 2048 else None
+        if args.families:
+            fams = args.families.split(",")
         from labeling_b200 import workloads as W
         inputs = make_2d_inputs(side, fams or W.FAMILIES_8192, seed=10 + 17 * rank)
         stages = STAGES_2D
@@ -552,6 +569,8 @@ def main():
     ap.add_argument("--workload", default="2d8192", choices=["2d8192", "2d2048", "3d512", "batch", "serve"])
     ap.add_argument("--rates", default="100,300,1000,3000,5000", help="serve: Poisson rates (req/s)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--families", default="", help="comma-separated subset of the workload's images "
+                    "(2D families, or 3D bern0.1,bern0.3,bern0.5,grf50,grf80), for profiling captures")
     ap.add_argument("--batch-images", type=int, default=4096)
     ap.add_argument("--pool", type=int, default=40, help="serve: pre-generated requests")
     args = ap.parse_args()
