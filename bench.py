@@ -327,15 +327,23 @@ def bench_ours(args, rank, world, local_rank):
                         "algorithmic_bytes": int(ab),
                         "achieved_gbs": round(ab / (ms / 1e3) / 1e9, 1) if ab and ms else None})
     dom = max(kernels, key=lambda k: k["ms"])
-    traffic = None
+    # DRAM traffic of one labeling from a committed ncu capture of the same workload's image size
+    # (profiles/traffic.json): the five launches' dram__bytes_read.sum + dram__bytes_write.sum.
+    traffic, traffic_note = None, None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         try:
-            traffic = json.load(open(tp)).get(args.workload)
+            tr = json.load(open(tp)).get(args.workload)
         except Exception:
-            traffic = None
+            tr = None
+        if tr:
+            traffic = int(tr["bytes_per_labeling"])
+            traffic_note = f"ncu, one {tr['image']} labeling, five launches"
+            for k in kernels:
+                k["traffic_bytes"] = tr["per_kernel"].get(k["kernel"])
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_note,
+                "algorithmic_bytes_per_labeling": int(5 * px_step),
                 "peak_kind": peak_kind, "scope": "whole labeling (5 launches), 5 B/px",
                 "dominant_kernel": dom["kernel"],
                 "frac_of_8tbs": round(achieved / 8000.0, 4)}
