@@ -43,6 +43,7 @@ constexpr int ZG = TB2 / 8;                 // 8-block groups along d2
 constexpr int ITEMS = TB0 * TB1 * ZG;       // items of 8 blocks
 constexpr int RBW = TZ / 32;                // root-bitmap words per voxel row
 constexpr uint32_t ROOT_FLAG = 1u << 23;
+constexpr int MQ3CAP = NBLK;                // merge-queue capacity (pairs per round)
 
 static_assert(NBLK <= (1 << 13), "tile-local block index must fit the entry payload");
 static_assert(TX * TY * TZ <= (1 << 23), "tile-local key must fit the entry payload");
@@ -182,12 +183,14 @@ __device__ __forceinline__ bool perim_pos3(int p, const TileGeo &g, int &f, int 
 __global__ void __launch_bounds__(NT, 4) k_tile_local_3d(ImgList3D L, Work w)
 {
     __shared__ uint32_t P[NBLK];
-    __shared__ uint32_t KM[NBLK];
+    __shared__ uint32_t KQ[NBLK];   // merge queue in Phase B, then first-voxel keys (KM)
+    uint32_t *const MQ3 = KQ, *const KM = KQ;
     __shared__ __align__(16) uint8_t M[NBLK];
     __shared__ uint32_t RB[TX * TY * RBW];
     __shared__ uint32_t BF[NBLK / 32];
     __shared__ uint32_t BP[NBLK / 32];
     __shared__ uint32_t tmp[NT / 32 + 1];
+    __shared__ uint32_t mqn3[4 * (ITEMS / NT)];      // queue length of each round
     __shared__ uint32_t qslot;
 
     const int tid = threadIdx.x;
@@ -200,8 +203,8 @@ __global__ void __launch_bounds__(NT, 4) k_tile_local_3d(ImgList3D L, Work w)
         const int64_t rs0 = int64_t(im.d1) * im.d2;   // stride of d0 in voxels
 
         for (int i = tid; i < TX * TY * RBW; i += NT) RB[i] = 0;
-        for (int i = tid; i < NBLK; i += NT) KM[i] = kNone;
         if (tid < NBLK / 32) BF[tid] = 0;
+        if (tid < 4 * (ITEMS / NT)) mqn3[tid] = 0;
 
         // Phase A: masks and runs along d2.
         uint64_t masks[ITEMS / NT];
@@ -249,63 +252,88 @@ __global__ void __launch_bounds__(NT, 4) k_tile_local_3d(ImgList3D L, Work w)
         // Phase B: merges with the 13 preceding neighbours inside the tile, decided for the 8
         // blocks of a group at once on byte-packed masks (bit 8k = block k): the 12 neighbours
         // in the four preceding rows (d0-1, d1-1 / d0-1, d1 / d0-1, d1+1 / d0, d1-1) and, at the
-        // group's first block, the block before it along d2.
+        // group's first block, the block before it along d2.  One round per (item, row): every
+        // lane queues its links in shared memory, then all lanes merge the queue, so lanes with
+        // many links do not hold up their warp.  A round queues at most NT * (3 * 8 + 1) pairs;
+        // the queue holds NBLK (it shares its memory with the keys of Phase C), and pairs beyond
+        // it are merged in place.
 #pragma unroll
-        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
+        for (int it_i = 0; it_i < ITEMS / NT; ++it_i)
+#pragma unroll 1
+        for (int row = 0; row < 4; ++row) {
+            const int round = 4 * it_i + row;
             const int it = tid + it_i * NT;
             const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
             const uint64_t ms = masks[it_i];
-            if (!ms) continue;
             const int bb = blk(b0, b1, 8 * zg);
-            const uint64_t ML = zg > 0 ? M[bb - 1] : 0u;
-            // hz: block k is joined along d2 to block k-1 (same run)
-            const uint64_t hz = nzb(ms & rep8(side_sel(0, 0, -1))) &
-                                nzb(((ms << 8) | ML) & rep8(side_sel(0, 0, 1)));
-            if (hz & 1u) merge_blocks3(P, bb, bb - 1);
-#pragma unroll 1
-            for (int row = 0; row < 4; ++row) {
-                const int dx = row < 3 ? -1 : 0, dy = row < 3 ? row - 1 : -1;
-                const int n0 = b0 + dx, n1 = b1 + dy;
-                if (n0 < 0 || n1 < 0 || n1 >= TB1) continue;
-                const int nb0 = blk(n0, n1, 8 * zg);
-                const uint2 nv = *reinterpret_cast<const uint2 *>(&M[nb0]);
-                const uint64_t N = (uint64_t(nv.y) << 32) | nv.x;
-                const uint64_t NL = zg > 0 ? M[nb0 - 1] : 0u;
-                const uint64_t NR = 8 * zg + 8 < TB2 ? M[nb0 + 8] : 0u;
-                if (!(N | NL | NR)) continue;
-                uint64_t c[3];
+            const int dx = row < 3 ? -1 : 0, dy = row < 3 ? row - 1 : -1;
+            const int n0 = b0 + dx, n1 = b1 + dy;
+            const int nb0 = (n0 >= 0 && n1 >= 0 && n1 < TB1) ? blk(n0, n1, 8 * zg) : -1;
+            uint64_t c[3] = {0, 0, 0};
+            bool link_z = false;
+            if (ms) {
+                const uint64_t ML = zg > 0 ? M[bb - 1] : 0u;
+                // hz: block k is joined along d2 to block k-1 (same run)
+                const uint64_t hz = nzb(ms & rep8(side_sel(0, 0, -1))) &
+                                    nzb(((ms << 8) | ML) & rep8(side_sel(0, 0, 1)));
+                link_z = row == 0 && (hz & 1u);
+                if (nb0 >= 0) {
+                    const uint2 nv = *reinterpret_cast<const uint2 *>(&M[nb0]);
+                    const uint64_t N = (uint64_t(nv.y) << 32) | nv.x;
+                    const uint64_t NL = zg > 0 ? M[nb0 - 1] : 0u;
+                    const uint64_t NR = 8 * zg + 8 < TB2 ? M[nb0 + 8] : 0u;
+                    if (N | NL | NR) {
 #pragma unroll
-                for (int dz = -1; dz <= 1; ++dz) {
-                    const uint64_t Ns = dz < 0 ? (N << 8) | NL : dz > 0 ? (N >> 8) | (NR << 56) : N;
-                    c[dz + 1] = nzb(ms & rep8(side_sel(dx, dy, dz))) & nzb(Ns & rep8(side_sel(-dx, -dy, -dz)));
-                }
-                // Skip rules (as in the 2D kernel: every chain of reasons runs toward smaller
-                // d2 along the run and ends at a link that is made).
-                // (1) The previous block of the run touches the same block of row N.
-                const uint64_t raw1 = c[1];
-                c[0] &= ~(hz & (raw1 << 8));
-                c[1] &= ~(hz & (c[2] << 8));
-                // (2) Blocks of row N joined along d2 to the block this one touches with dz = 0.
-                const uint64_t hzN = nzb(N & rep8(side_sel(0, 0, -1))) &
-                                     nzb(((N << 8) | NL) & rep8(side_sel(0, 0, 1)));
-                const uint64_t hzN1 = (hzN >> 8) |
-                                      (uint64_t((NR & side_sel(0, 0, -1)) && ((N >> 56) & side_sel(0, 0, 1))) << 56);
-                c[0] &= ~(raw1 & hzN);
-                c[2] &= ~(raw1 & hzN1);
-                uint64_t todo = c[0] | c[1] | c[2];
-                while (todo) {
-                    const int k = (__ffsll(todo) - 1) >> 3;
-                    const uint64_t bit = uint64_t(1) << (8 * k);
-                    todo &= ~bit;
-                    if (c[0] & bit) merge_blocks3(P, bb + k, nb0 + k - 1);
-                    if (c[1] & bit) merge_blocks3(P, bb + k, nb0 + k);
-                    if (c[2] & bit) merge_blocks3(P, bb + k, nb0 + k + 1);
+                        for (int dz = -1; dz <= 1; ++dz) {
+                            const uint64_t Ns = dz < 0 ? (N << 8) | NL : dz > 0 ? (N >> 8) | (NR << 56) : N;
+                            c[dz + 1] = nzb(ms & rep8(side_sel(dx, dy, dz))) &
+                                        nzb(Ns & rep8(side_sel(-dx, -dy, -dz)));
+                        }
+                        // Skip rules (as in the 2D kernel: every chain of reasons runs toward
+                        // smaller d2 along the run and ends at a link that is made).
+                        // (1) The previous block of the run touches the same block of row N.
+                        const uint64_t raw1 = c[1];
+                        c[0] &= ~(hz & (raw1 << 8));
+                        c[1] &= ~(hz & (c[2] << 8));
+                        // (2) Blocks of row N joined along d2 to the block this one touches
+                        //     with dz = 0.
+                        const uint64_t hzN = nzb(N & rep8(side_sel(0, 0, -1))) &
+                                             nzb(((N << 8) | NL) & rep8(side_sel(0, 0, 1)));
+                        const uint64_t hzN1 =
+                            (hzN >> 8) |
+                            (uint64_t((NR & side_sel(0, 0, -1)) && ((N >> 56) & side_sel(0, 0, 1))) << 56);
+                        c[0] &= ~(raw1 & hzN);
+                        c[2] &= ~(raw1 & hzN1);
+                    }
                 }
             }
+            const uint32_t n = __popcll(c[0]) + __popcll(c[1]) + __popcll(c[2]) + (link_z ? 1u : 0u);
+            uint32_t pos = warp_reserve(&mqn3[round], n);
+            auto push = [&](uint32_t x, uint32_t y) {
+                if (pos < uint32_t(MQ3CAP)) MQ3[pos] = (x << 16) | y;
+                else smerge(P, x, y);   // queue full: merge in place
+                ++pos;
+            };
+            if (link_z) push(uint32_t(bb), uint32_t(bb - 1));
+            uint64_t todo = c[0] | c[1] | c[2];
+            while (todo) {
+                const int k = (__ffsll(todo) - 1) >> 3;
+                const uint64_t bit = uint64_t(1) << (8 * k);
+                todo &= ~bit;
+                if (c[0] & bit) push(uint32_t(bb + k), uint32_t(nb0 + k - 1));
+                if (c[1] & bit) push(uint32_t(bb + k), uint32_t(nb0 + k));
+                if (c[2] & bit) push(uint32_t(bb + k), uint32_t(nb0 + k + 1));
+            }
+            __syncthreads();
+            const uint32_t nq = min(mqn3[round], uint32_t(MQ3CAP));
+            for (uint32_t q = tid; q < nq; q += NT) smerge(P, MQ3[q] >> 16, MQ3[q] & 0xFFFFu);
+            __syncthreads();
         }
-        __syncthreads();
 
-        // Phase C: roots (read-only finds: all merges are done) and per-component first-voxel key.
+        // Phase C: roots (read-only finds: all merges are done) and per-component first-voxel
+        // key.  Each root first stores its own block's key; a block of the component then needs
+        // the atomic only when its key is smaller, which keeps the atomics off the (common) case
+        // of a large component whose blocks all follow its root block.
         uint16_t roots[ITEMS / NT][8];
 #pragma unroll
         for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
@@ -317,9 +345,26 @@ __global__ void __launch_bounds__(NT, 4) k_tile_local_3d(ImgList3D L, Work w)
                 const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
                 if (!m) continue;
                 const int b = blk(b0, b1, 8 * zg + k);
-                const uint32_t root = sfind_ro(P, b);
+                const uint32_t root = sflatten(P, b);
                 roots[it_i][k] = uint16_t(root);
-                atomicMin(&KM[root], local_key(b, m));
+                if (root == uint32_t(b)) KM[b] = local_key(b, m);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
+            const int it = tid + it_i * NT;
+            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
+            const uint64_t ms = masks[it_i];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
+                if (!m) continue;
+                const int b = blk(b0, b1, 8 * zg + k);
+                const uint32_t root = roots[it_i][k];
+                if (root == uint32_t(b)) continue;
+                const uint32_t key = local_key(b, m);
+                if (key < KM[root]) atomicMin(&KM[root], key);
             }
         }
         __syncthreads();
