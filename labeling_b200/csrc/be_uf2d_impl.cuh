@@ -378,10 +378,17 @@ __device__ void gunion2d(const Img2D &im, Work &w, uint32_t a, uint32_t b)
 }  // namespace
 
 constexpr int K2_NT = TBH + TBW;
+constexpr int kFilterSlots2 = 2048;
+constexpr int kGQ2 = 512;   // queued global unions per tile (more are done at once)
 
+// One thread per right-border and bottom-border position.  Every connected pair goes through the
+// CTA-local node filter (NodeFilter, be_common.cuh); the pairs that join two local sets are
+// unioned globally from a shared queue once the tile's pairs are all seen.
 __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
 {
     __shared__ uint32_t qslot;
+    __shared__ NodeFilter<kFilterSlots2> flt;
+    __shared__ uint2 gq[kGQ2];
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
         const Img2D im = L.get(t);
@@ -391,59 +398,71 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
         const int nbc = (min(TW, im.cols - tx * TW) + 1) >> 1;
         const int p = threadIdx.x;
         const uint16_t *pe = w.perim;
+        filter_reset(flt);
+        __syncthreads();
+        auto pair = [&](uint32_t nA, uint32_t nB) {
+            if (!filter_pair(flt, nA, nB)) return;
+            const uint32_t slot = atomicAdd(&flt.nq, 1u);
+            if (slot < uint32_t(kGQ2)) gq[slot] = make_uint2(nA, nB);
+            else gunion2d(im, w, nA, nB);
+        };
         if (p < TBH) {
             // Right border: neighbours in the tile to the right, same tile row.
             const int r = p;
-            if (r >= nbr || tx + 1 >= im.tiles_x) continue;
-            const uint32_t A = pe[t * NPERIM + 2 * TBW + TBH + r];
-            if (!A) continue;
-            const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
-            const int64_t t2 = t + 1;
-            uint32_t last = kNone;
+            const uint32_t A = (r < nbr && tx + 1 < im.tiles_x) ? pe[t * NPERIM + 2 * TBW + TBH + r] : 0u;
+            if (A) {
+                const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
+                const int64_t t2 = t + 1;
+                uint32_t last = kNone;
 #pragma unroll
-            for (int d = -1; d <= 1; ++d) {
-                const int rr = r + d;
-                if (rr < 0 || rr >= nbr) continue;
-                const uint32_t B = pe[t2 * NPERIM + 2 * TBW + rr];
-                if (!B) continue;
-                const uint32_t mB = B & 15u;
-                const bool c = d == 0 ? ((mA & 0xAu) && (mB & 0x5u))
-                                      : d < 0 ? ((mA & 2u) && (mB & 4u)) : ((mA & 8u) && (mB & 1u));
-                const uint32_t nB = uint32_t(t2 * MAXB + (B >> 4));
-                if (c && nB != last) gunion2d(im, w, nA, nB);
-                if (c) last = nB;
+                for (int d = -1; d <= 1; ++d) {
+                    const int rr = r + d;
+                    if (rr < 0 || rr >= nbr) continue;
+                    const uint32_t B = pe[t2 * NPERIM + 2 * TBW + rr];
+                    if (!B) continue;
+                    const uint32_t mB = B & 15u;
+                    const bool c = d == 0 ? ((mA & 0xAu) && (mB & 0x5u))
+                                          : d < 0 ? ((mA & 2u) && (mB & 4u)) : ((mA & 8u) && (mB & 1u));
+                    const uint32_t nB = uint32_t(t2 * MAXB + (B >> 4));
+                    if (c && nB != last) pair(nA, nB);
+                    if (c) last = nB;
+                }
             }
         } else {
             // Bottom border: neighbours in the tile row below (including the diagonal tiles).
             const int c = p - TBH;
-            if (c >= nbc || ty + 1 >= im.tiles_y) continue;
-            const uint32_t A = pe[t * NPERIM + TBW + c];
-            if (!A) continue;
-            const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
-            uint32_t last = kNone;
+            const uint32_t A = (c < nbc && ty + 1 < im.tiles_y) ? pe[t * NPERIM + TBW + c] : 0u;
+            if (A) {
+                const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
+                uint32_t last = kNone;
 #pragma unroll
-            for (int d = -1; d <= 1; ++d) {
-                int cc = c + d;
-                int64_t t2 = t + im.tiles_x;
-                if (cc < 0) {
-                    if (tx == 0) continue;
-                    t2 -= 1;
-                    cc = TBW - 1;
-                } else if (cc >= nbc) {
-                    if (tx + 1 >= im.tiles_x) continue;
-                    t2 += 1;
-                    cc = 0;
+                for (int d = -1; d <= 1; ++d) {
+                    int cc = c + d;
+                    int64_t t2 = t + im.tiles_x;
+                    if (cc < 0) {
+                        if (tx == 0) continue;
+                        t2 -= 1;
+                        cc = TBW - 1;
+                    } else if (cc >= nbc) {
+                        if (tx + 1 >= im.tiles_x) continue;
+                        t2 += 1;
+                        cc = 0;
+                    }
+                    const uint32_t B = pe[t2 * NPERIM + cc];
+                    if (!B) continue;
+                    const uint32_t mB = B & 15u;
+                    const bool cn = d == 0 ? ((mA & 0xCu) && (mB & 0x3u))
+                                           : d < 0 ? ((mA & 4u) && (mB & 2u)) : ((mA & 8u) && (mB & 1u));
+                    const uint32_t nB = uint32_t(t2 * MAXB + (B >> 4));
+                    if (cn && nB != last) pair(nA, nB);
+                    if (cn) last = nB;
                 }
-                const uint32_t B = pe[t2 * NPERIM + cc];
-                if (!B) continue;
-                const uint32_t mB = B & 15u;
-                const bool cn = d == 0 ? ((mA & 0xCu) && (mB & 0x3u))
-                                       : d < 0 ? ((mA & 4u) && (mB & 2u)) : ((mA & 8u) && (mB & 1u));
-                const uint32_t nB = uint32_t(t2 * MAXB + (B >> 4));
-                if (cn && nB != last) gunion2d(im, w, nA, nB);
-                if (cn) last = nB;
             }
         }
+        __syncthreads();
+        const uint32_t nq = min(flt.nq, uint32_t(kGQ2));
+        for (uint32_t i = threadIdx.x; i < nq; i += K2_NT) gunion2d(im, w, gq[i].x, gq[i].y);
+        __syncthreads();
     }
 }
 

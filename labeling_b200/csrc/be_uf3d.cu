@@ -488,27 +488,18 @@ __device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
 
 }  // namespace
 
-// Per-CTA set of node pairs already unioned for the current tile (open addressing on 64-bit
-// keys); dense volumes produce the same pair from hundreds of face blocks.
-constexpr int kPairSlots = 2048;
+// Cross-tile pairs go through a CTA-local node filter (be_common.cuh: NodeFilter) and only the
+// pairs that join two local sets are unioned globally, from a shared queue after all pairs of
+// the tile are seen; dense volumes produce the same few border components from hundreds of face
+// blocks.
+constexpr int kFilterSlots3 = 4096;
+constexpr int kGQ3 = 1024;   // queued global unions per tile (more are done at once)
 
-__device__ __forceinline__ bool pair_first_seen(unsigned long long *set, uint32_t a, uint32_t b)
-{
-    const unsigned long long key = (uint64_t(a) << 32) | b;
-    uint32_t h = (a * 0x9E3779B1u) ^ (b * 0x85EBCA77u);
-    for (int probe = 0; probe < 8; ++probe) {
-        const uint32_t i = (h + probe) & (kPairSlots - 1);
-        const unsigned long long old = atomicCAS(&set[i], ~0ull, key);
-        if (old == ~0ull) return true;   // inserted: first occurrence
-        if (old == key) return false;    // already done by another thread
-    }
-    return true;                         // table crowded: just do the union
-}
-
-__global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work w)
+__global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Work w)
 {
     __shared__ uint32_t qslot;
-    __shared__ unsigned long long pairs[kPairSlots];
+    __shared__ NodeFilter<kFilterSlots3> flt;
+    __shared__ uint2 gq[kGQ3];
     constexpr int NPLUS = TB1 * TB2 + TB0 * TB2 + TB0 * TB1;
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
@@ -518,7 +509,7 @@ __global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work 
         const int tb[3] = {TB0, TB1, TB2};
         const int tc[3] = {g.tx0, g.tx1, g.tx2};
         const int tn[3] = {im.t0, im.t1, im.t2};
-        for (int i = threadIdx.x; i < kPairSlots; i += kT3MergeThreads) pairs[i] = ~0ull;
+        filter_reset(flt);
         __syncthreads();
         for (int p = threadIdx.x; p < NPLUS; p += kT3MergeThreads) {
             int axis, q;
@@ -537,8 +528,7 @@ __global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work 
             const uint32_t fa = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
             if (!GUARD(w, (A >> 4) < w.nb[t], 204, (uint64_t(t) << 16) | (A >> 4))) continue;
             const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;   // tangent axes in order
-            uint32_t done[9];
-            int ndone = 0;
+            uint32_t last = kNone;
             for (int da = -1; da <= 1; ++da) {
                 for (int db = -1; db <= 1; ++db) {
                     if (!(fa & face_sel(da, db))) continue;
@@ -558,14 +548,18 @@ __global__ void __launch_bounds__(kT3MergeThreads) k_merge_3d(ImgList3D L, Work 
                     if (!((B & 15u) & face_sel(-da, -db))) continue;
                     const uint32_t nB = uint32_t(t2i * MAXB + (B >> 4));
                     if (!GUARD(w, (B >> 4) < w.nb[t2i], 203, (uint64_t(t2i) << 16) | (B >> 4))) continue;
-                    bool seen = false;
-                    for (int q2 = 0; q2 < ndone; ++q2) seen |= done[q2] == nB;
-                    if (seen) continue;
-                    done[ndone++] = nB;
-                    if (pair_first_seen(pairs, nA, nB)) gunion3d(im, w, nA, nB);
+                    if (nB == last) continue;
+                    last = nB;
+                    if (!filter_pair(flt, nA, nB)) continue;
+                    const uint32_t slot = atomicAdd(&flt.nq, 1u);
+                    if (slot < uint32_t(kGQ3)) gq[slot] = make_uint2(nA, nB);
+                    else gunion3d(im, w, nA, nB);
                 }
             }
         }
+        __syncthreads();
+        const uint32_t nq = min(flt.nq, uint32_t(kGQ3));
+        for (uint32_t i = threadIdx.x; i < nq; i += kT3MergeThreads) gunion3d(im, w, gq[i].x, gq[i].y);
         __syncthreads();
     }
 }
