@@ -80,7 +80,7 @@ struct Work {
     int32_t n_imgs;
 };
 
-constexpr int kScanChunk = 16384;   // segments per scan chunk (one CTA)
+constexpr int kScanChunk = 4096;    // segments per scan chunk (one CTA)
 
 // ---------------------------------------------------------------------------------------------
 // Bounds-checked build (-DBE_BOUNDS_CHECK): GUARD(w, cond, site, value) is false when `cond`
@@ -341,10 +341,7 @@ __device__ __forceinline__ int filter_slot(NodeFilter<KH> &f, uint32_t n)
 {
     uint32_t h = (n * 2654435761u) & uint32_t(KH - 1);
     for (int probe = 0; probe < 32; ++probe) {
-        // Plain read first: most lookups find a key that is already there, and a CAS on it from
-        // every lane of a dense tile would serialise on one address.
-        uint32_t old = *reinterpret_cast<volatile uint32_t *>(&f.key[h]);
-        if (old == kNone) old = atomicCAS(&f.key[h], kNone, n);
+        const uint32_t old = atomicCAS(&f.key[h], kNone, n);
         if (old == kNone || old == n) return int(h);
         h = (h + 1) & uint32_t(KH - 1);
     }

@@ -10,7 +10,7 @@ namespace be {
 __global__ void __launch_bounds__(kScanThreads) k_segscan(Work w)
 {
     constexpr int NT = kScanThreads;
-    constexpr int PER = kScanChunk / NT;   // 64 counts per thread
+    constexpr int PER = kScanChunk / NT;   // 16 counts per thread
     __shared__ uint32_t tmp[NT / 32 + 1];
     const int64_t c = blockIdx.x;
     uint32_t off = 0;

@@ -7,18 +7,22 @@ constexpr int TW = 2 * TBW, TH = 2 * TBH;          // tile in pixels
 constexpr int NBLK = TBW * TBH;                    // blocks per tile (4096)
 constexpr int NPERIM = 2 * (TBW + TBH);            // border positions per tile
 constexpr int MAXB = NPERIM;                       // nodes per tile
-constexpr int K1_NT = 256;
-constexpr int ITEMS = NBLK / 8;                    // 8-block row groups per tile
-constexpr int GROUPS = TBW / 8;                    // groups per block row
-constexpr int MQCAP = 2048;                        // merge-queue capacity (pairs per tile)
+constexpr int WPR = TBW / 32;                      // 32-block words per block row
+constexpr int K1_NT = TBH * WPR;                   // one thread per (block row, word) = NBLK / 32
+constexpr int MQCAP = NBLK;                        // merge-queue capacity (links per tile)
+constexpr uint32_t kPass = 0xFFFFu;                // "no run start" in the carry scan
 
 static_assert(NBLK <= 4096, "tile-local block index must fit 12 bits");
 static_assert(MAXB < 4096, "node index must fit 12 bits");
+static_assert(K1_NT == NBLK / 32 && (WPR & (WPR - 1)) == 0 && WPR <= 32, "thread layout");
 
-// Mask bits: 0 = top-left, 1 = top-right, 2 = bottom-left, 3 = bottom-right pixel.
-__device__ __forceinline__ uint32_t slot_of(int r, int c, uint32_t m)
+// Union-find slot order of a block: r*2*TBW + t*TBW + c with t = 0 when the block has a pixel in
+// its top row.  The order is the raster order of the blocks' first pixels, so the smallest slot
+// of a component is the block holding its first pixel.  Mask bits: 0 = top-left, 1 = top-right,
+// 2 = bottom-left, 3 = bottom-right pixel.
+__device__ __forceinline__ uint32_t key_block(uint32_t key)
 {
-    return uint32_t(r) * (2 * TBW) + ((m & 3u) ? 0u : uint32_t(TBW)) + uint32_t(c);
+    return (key / (2 * TBW)) * TBW + (key % TBW);
 }
 
 // Pixel offset (row, column) of a block's first foreground pixel, inside the block.
@@ -26,11 +30,6 @@ __device__ __forceinline__ void first_px(uint32_t m, int &dy, int &dx)
 {
     if (m & 3u) { dy = 0; dx = (m & 1u) ? 0 : 1; }
     else { dy = 1; dx = (m & 4u) ? 0 : 1; }
-}
-
-__device__ __forceinline__ bool hconn(uint32_t left, uint32_t right)
-{
-    return (left & 0xAu) && (right & 0x5u);
 }
 
 // Block position of border position p of a tile with nbr x nbc valid blocks.
@@ -43,48 +42,103 @@ __device__ __forceinline__ bool perim_pos(int p, int nbr, int nbc, int &r, int &
     return r < nbr;
 }
 
-// Nibble-packed mask words: nibble k = mask of block k; nb_bN gives bit N of every nibble at
-// bit 4k, so block-wise predicates of 8 blocks are a few bitwise operations.
-__device__ __forceinline__ uint32_t nb_b0(uint32_t x) { return x & 0x11111111u; }
-__device__ __forceinline__ uint32_t nb_b1(uint32_t x) { return (x >> 1) & 0x11111111u; }
-__device__ __forceinline__ uint32_t nb_b2(uint32_t x) { return (x >> 2) & 0x11111111u; }
-__device__ __forceinline__ uint32_t nb_b3(uint32_t x) { return (x >> 3) & 0x11111111u; }
-__device__ __forceinline__ uint32_t nb_lft(uint32_t x) { return nb_b0(x) | nb_b2(x); }
-__device__ __forceinline__ uint32_t nb_rgt(uint32_t x) { return nb_b1(x) | nb_b3(x); }
-
-// Four bytes (each < 16) -> four nibbles.
-__device__ __forceinline__ uint32_t bytes_to_nibbles(uint32_t x)
+// Byte-wise x > thr for four pixels: bit 7 of each byte.  K = 0x7F - (thr & 0x7F) in every byte;
+// `hi` = thr >= 128.  (x & 0x7F) + K carries into bit 7 exactly when the low seven bits exceed
+// thr's; the high bit decides the rest.
+__device__ __forceinline__ uint32_t gt_bytes(uint32_t x, uint32_t K, bool hi)
 {
-    x = (x | (x >> 4)) & 0x00FF00FFu;
-    return (x | (x >> 8)) & 0xFFFFu;
+    const uint32_t s = (x & 0x7F7F7F7Fu) + K;
+    return (hi ? (x & s) : (x | s)) & 0x80808080u;
 }
 
-__device__ __forceinline__ uint32_t nib2byte(uint32_t x)
+// Bits 7, 15, 23, 31 -> bits 0..3 (the four partial products land on distinct bits, no carries).
+__device__ __forceinline__ uint32_t gather4(uint32_t g) { return (g * 0x00204081u) >> 28; }
+
+// 16 pixels of one row -> foreground bits of their even (left) and odd (right) pixels: 8 blocks.
+__device__ __forceinline__ void split16(uint4 v, uint32_t K, bool hi, uint32_t &ev, uint32_t &od)
 {
-    x &= 0xFFFFu;
-    x = (x | (x << 8)) & 0x00FF00FFu;
-    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    ev = gather4(gt_bytes(__byte_perm(v.x, v.y, 0x6420), K, hi)) |
+         (gather4(gt_bytes(__byte_perm(v.z, v.w, 0x6420), K, hi)) << 4);
+    od = gather4(gt_bytes(__byte_perm(v.x, v.y, 0x7531), K, hi)) |
+         (gather4(gt_bytes(__byte_perm(v.z, v.w, 0x7531), K, hi)) << 4);
+}
+
+// Bits 0..3 of x -> bit 0 of bytes 0..3.
+__device__ __forceinline__ uint32_t spread4(uint32_t x) { return ((x & 0xFu) * 0x00204081u) & 0x01010101u; }
+
+// Highest set bit of x (x != 0).
+__device__ __forceinline__ uint32_t hibit(uint32_t x) { return 31u - __clz(x); }
+
+// Union-find over run starts with the slot order carried in the parent entry: P[x] holds
+// (slot << 12) | parent, and a root holds its own (slot << 12) | x.  Entries only ever decrease,
+// so the union (atomicMin of the smaller encoding into the other root, Playne-Hawick style)
+// leaves the run with the smallest slot -- the component's first pixel -- as the root.
+__device__ __forceinline__ uint32_t efind(uint32_t *P, uint32_t x)
+{
+    uint32_t v = P[x];
+    while ((v & 0xFFFu) != x) {
+        const uint32_t y = v & 0xFFFu;
+        const uint32_t vg = P[y];
+        if ((vg & 0xFFFu) != y) P[x] = vg;   // path halving
+        x = y;
+        v = vg;
+    }
     return x;
+}
+
+__device__ __forceinline__ uint32_t efind_ro(const uint32_t *P, uint32_t x)
+{
+    uint32_t v = P[x];
+    while ((v & 0xFFFu) != x) {
+        x = v & 0xFFFu;
+        v = P[x];
+    }
+    return x;
+}
+
+__device__ __forceinline__ void eunion(uint32_t *P, uint32_t a, uint32_t b)
+{
+    for (;;) {
+        a = efind(P, a);
+        b = efind(P, b);
+        if (a == b) return;
+        const uint32_t ea = P[a], eb = P[b];
+        if (ea < eb) {
+            const uint32_t old = atomicMin(&P[b], ea);
+            if ((old & 0xFFFu) == b) return;
+            b = old & 0xFFFu;
+        } else {
+            const uint32_t old = atomicMin(&P[a], eb);
+            if ((old & 0xFFFu) == a) return;
+            a = old & 0xFFFu;
+        }
+    }
 }
 
 }  // namespace
 
 // ---------------------------------------------------------------------------------------------
-// Tile-local labeling.
+// Tile-local labeling.  One thread per 32 blocks of a block row (a "word"): the four pixel
+// classes of the blocks (top-left, top-right, bottom-left, bottom-right) are 32-bit words, so
+// horizontal runs of joined blocks, their starts and the links to the row above are bitwise
+// operations; only runs enter the union-find, and only links between runs that no earlier link
+// already joins are merged.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
+__global__ void __launch_bounds__(K1_NT, 5) k_tile_local_2d(ImgList2D L, Work w)
 {
-    __shared__ uint32_t P[2 * NBLK];
+    __shared__ uint32_t P[NBLK];            // run starts: (slot << 12) | parent
     __shared__ __align__(16) uint8_t M[NBLK];
+    __shared__ uint32_t WBL[NBLK / 32], WBR[NBLK / 32], WHC[NBLK / 32], WS[NBLK / 32], WCS[NBLK / 32];
     __shared__ uint32_t RB[TH][TW / 32];
     __shared__ uint32_t BF[NBLK / 32];
     __shared__ uint32_t BP[NBLK / 32];
-    __shared__ uint32_t MQ[MQCAP];          // merge queue: (slot_a << 16) | slot_b
-    __shared__ uint32_t mqn[2];
+    __shared__ uint32_t MQ[MQCAP];          // merge queue: (start_a << 16) | start_b
+    __shared__ uint32_t mqn;
     __shared__ uint32_t tmp[K1_NT / 32 + 1];
     __shared__ uint32_t qslot;
 
     const int tid = threadIdx.x;
+    const int r = tid / WPR, q = tid % WPR;
     uint16_t *lab = reinterpret_cast<uint16_t *>(w.lab);
     ItemLoop loop{w.queue ? w.queue + 0 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
@@ -94,200 +148,248 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
         const int y0 = ty * TH, x0 = tx * TW;
         const int nrp = min(TH, im.rows - y0), ncp = min(TW, im.cols - x0);
         const int nbr = (nrp + 1) >> 1, nbc = (ncp + 1) >> 1;
-        const uint32_t thr4 = uint32_t(im.thr) * 0x01010101u;
+        const uint32_t K = (0x7Fu - (uint32_t(im.thr) & 0x7Fu)) * 0x01010101u;
+        const bool hi = im.thr >= 128;
 
         for (int i = tid; i < TH * (TW / 32); i += K1_NT) (&RB[0][0])[i] = 0;
-        if (tid < NBLK / 32) BF[tid] = 0;
-        if (tid < 2) mqn[tid] = 0;
+        BF[tid] = 0;
+        if (tid == 0) mqn = 0;
 
-        // Phase A: load pixels, build block masks, seed the union-find with horizontal runs.
-        uint32_t masks[ITEMS / K1_NT];
+        // Phase A: pixel words, runs, run starts and their slots.
+        uint32_t TLw = 0, TRw = 0, BLw = 0, BRw = 0;
+        if (r < nbr && 64 * q < ncp) {
+            const uint8_t *row0 = im.in + int64_t(y0 + 2 * r) * im.in_pitch + x0 + 64 * q;
+            const bool row1 = 2 * r + 1 < nrp;
+            const bool vec = (64 * q + 64 <= ncp) &&
+                             ((reinterpret_cast<uintptr_t>(row0) | uintptr_t(im.in_pitch)) & 15) == 0;
+            if (vec) {
+                const uint4 *p0 = reinterpret_cast<const uint4 *>(row0);
+                uint4 v[4], u[4];
 #pragma unroll
-        for (int i = 0; i < ITEMS / K1_NT; ++i) {
-            const int it = tid + i * K1_NT, r = it / GROUPS, g = it % GROUPS;
-            uint32_t top = 0, bot = 0;
-            if (r < nbr && 16 * g < ncp) {
-                const int py = y0 + 2 * r, px = x0 + 16 * g;
-                const uint8_t *row0 = im.in + int64_t(py) * im.in_pitch + px;
-                const bool row1 = py + 1 < im.rows;
-                const bool vec = (16 * g + 16 <= ncp) &&
-                                 ((reinterpret_cast<uintptr_t>(row0) | uintptr_t(im.in_pitch)) & 15) == 0;
-                if (vec) {
-                    top = fg16(__ldg(reinterpret_cast<const uint4 *>(row0)), thr4);
-                    if (row1) bot = fg16(__ldg(reinterpret_cast<const uint4 *>(row0 + im.in_pitch)), thr4);
-                } else {
-                    const int n = min(16, ncp - 16 * g);
-                    for (int x = 0; x < n; ++x) {
-                        top |= uint32_t(row0[x] > im.thr) << x;
-                        if (row1) bot |= uint32_t(row0[im.in_pitch + x] > im.thr) << x;
+                for (int i = 0; i < 4; ++i) v[i] = __ldg(p0 + i);
+                if (row1) {
+                    const uint4 *p1 = reinterpret_cast<const uint4 *>(row0 + im.in_pitch);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) u[i] = __ldg(p1 + i);
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    uint32_t ev, od;
+                    split16(v[i], K, hi, ev, od);
+                    TLw |= ev << (8 * i);
+                    TRw |= od << (8 * i);
+                    if (row1) {
+                        split16(u[i], K, hi, ev, od);
+                        BLw |= ev << (8 * i);
+                        BRw |= od << (8 * i);
                     }
                 }
+            } else {
+                const int n = min(64, ncp - 64 * q);
+                for (int x = 0; x < n; ++x) {
+                    const uint32_t bt = uint32_t(row0[x] > im.thr) << (x >> 1);
+                    const uint32_t bb = row1 ? uint32_t(row0[im.in_pitch + x] > im.thr) << (x >> 1) : 0u;
+                    if (x & 1) { TRw |= bt; BRw |= bb; }
+                    else { TLw |= bt; BLw |= bb; }
+                }
             }
-            const uint32_t ms = pairs_to_nibbles(top) | (pairs_to_nibbles(bot) << 2);
-            masks[i] = ms;
-            *reinterpret_cast<uint2 *>(&M[r * TBW + 8 * g]) = make_uint2(nib2byte(ms), nib2byte(ms >> 16));
-            // Horizontal runs: every block points at its run's smallest slot.  Within the group
-            // a prefix minimum finds each run part's minimum; runs that cross group borders are
-            // joined with segmented minimum scans over the 16 groups of the block row (one
-            // half-warp), so no merge is needed for horizontal links.
-            uint32_t pm[8];
-            bool inf[8];
+        }
+        const uint32_t Lw = TLw | BLw, Rw = TRw | BRw, Tw = TLw | TRw, Fw = Tw | BLw | BRw;
+        // hc bit k: block k is joined to block k + 1 (a right pixel of k touches a left pixel of
+        // k + 1 -- every such pair is 8-adjacent); bit 31 looks at the next word.
+        const uint32_t Lnext = __shfl_down_sync(0xFFFFFFFFu, Lw, 1, WPR);
+        const uint32_t hc = (Rw & (Lw >> 1)) | ((q + 1 < WPR) ? (Rw & (Lnext << 31)) : 0u);
+        const uint32_t hcprev = __shfl_up_sync(0xFFFFFFFFu, hc, 1, WPR);
+        const uint32_t cin = q > 0 ? (hcprev >> 31) : 0u;   // block 0 continues a run from the left
+        const uint32_t hl = (hc << 1) | cin;                  // bit k: block k joined to block k - 1
+        const uint32_t S = Fw & ~hl;                          // run starts
+        // Column of the start of the run entering from the left: the last start among the words
+        // before this one (an inclusive "last start" scan over the row's words).
+        uint32_t v = S ? uint32_t(32 * q) + hibit(S) : kPass;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t m = (ms >> (4 * k)) & 15u;
-                const uint32_t s = slot_of(r, 8 * g + k, m);
-                const bool hc = k > 0 && hconn((ms >> (4 * (k - 1))) & 15u, m);
-                pm[k] = hc ? min(pm[k - 1], s) : s;
-                inf[k] = k == 0 ? (m != 0) : (inf[k - 1] && hc);
-            }
-            const uint32_t m0 = ms & 15u, m7 = ms >> 28;
-            const uint32_t prev_ms = __shfl_up_sync(0xFFFFFFFFu, ms, 1, GROUPS);
-            const bool linkL = g > 0 && hconn(prev_ms >> 28, m0);
-            const bool linkR = __shfl_down_sync(0xFFFFFFFFu, uint32_t(linkL), 1, GROUPS) && g + 1 < GROUPS;
-            const bool single = inf[7];
-            // first_min: minimum of the run part holding block 0 (found by the backward pass).
-            uint32_t run = kNone, first_min = kNone;
-            uint32_t part[8];
+        for (int o = 1; o < WPR; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, v, o, WPR);
+            if (q >= o && v == kPass) v = u;
+        }
+        const uint32_t vprev = __shfl_up_sync(0xFFFFFFFFu, v, 1, WPR);
+        const uint32_t CSc = cin ? vprev : kPass;
+        const uint32_t rbase = uint32_t(r) * TBW, sbase = uint32_t(r) * (2 * TBW);
+
+        // Block masks as bytes (for the first-pixel lookups and the border entries).
+        uint32_t mw[8];
 #pragma unroll
-            for (int k = 7; k >= 0; --k) {
-                const uint32_t m = (ms >> (4 * k)) & 15u;
-                const bool last = (k == 7) || !hconn(m, (ms >> (4 * (k + 1))) & 15u);
-                if (last) run = pm[k];
-                part[k] = run;
-            }
-            first_min = m0 ? part[0] : kNone;
-            const uint32_t last_min = m7 ? pm[7] : kNone;
-            // Left-to-right: minimum of the run entering from the left.
-            uint32_t fv = last_min;
-            uint32_t ff = !(single && linkL);
-#pragma unroll
-            for (int o = 1; o < GROUPS; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, fv, o, GROUPS);
-                const uint32_t f = __shfl_up_sync(0xFFFFFFFFu, ff, o, GROUPS);
-                if (g >= o && !ff) { fv = min(fv, v); ff |= f; }
-            }
-            const uint32_t fprev = __shfl_up_sync(0xFFFFFFFFu, fv, 1, GROUPS);
-            const uint32_t fromL = linkL ? fprev : kNone;
-            // Right-to-left: minimum of the run leaving to the right.
-            uint32_t bv = first_min;
-            uint32_t bf = !(single && linkR);
-#pragma unroll
-            for (int o = 1; o < GROUPS; o <<= 1) {
-                const uint32_t v = __shfl_down_sync(0xFFFFFFFFu, bv, o, GROUPS);
-                const uint32_t f = __shfl_down_sync(0xFFFFFFFFu, bf, o, GROUPS);
-                if (g + o < GROUPS && !bf) { bv = min(bv, v); bf |= f; }
-            }
-            const uint32_t bnext = __shfl_down_sync(0xFFFFFFFFu, bv, 1, GROUPS);
-            const uint32_t fromR = linkR ? bnext : kNone;
-            bool inl = m7 != 0;
-#pragma unroll
-            for (int k = 7; k >= 0; --k) {
-                const uint32_t m = (ms >> (4 * k)) & 15u;
-                if (k < 7) inl = inl && hconn(m, (ms >> (4 * (k + 1))) & 15u);
-                if (!m) continue;
-                uint32_t v = part[k];
-                if (inf[k]) v = min(v, fromL);
-                if (inl) v = min(v, fromR);
-                P[slot_of(r, 8 * g + k, m)] = v;
+        for (int i = 0; i < 8; ++i) {
+            const int k = 4 * i;
+            mw[i] = spread4(TLw >> k) | (spread4(TRw >> k) << 1) | (spread4(BLw >> k) << 2) |
+                    (spread4(BRw >> k) << 3);
+        }
+        {
+            uint4 *mdst = reinterpret_cast<uint4 *>(&M[rbase + 32 * q]);
+            mdst[0] = make_uint4(mw[0], mw[1], mw[2], mw[3]);
+            mdst[1] = make_uint4(mw[4], mw[5], mw[6], mw[7]);
+        }
+        WBL[tid] = BLw;
+        WBR[tid] = BRw;
+        WHC[tid] = hc;
+        WS[tid] = S;
+        WCS[tid] = CSc;
+        // Slots of the runs that start here: the first block with a top pixel, else the start.
+        {
+            uint32_t ss = S;
+            while (ss) {
+                const uint32_t s0 = __ffs(ss) - 1;
+                ss &= ss - 1;
+                const uint32_t from = ~0u << s0;
+                const uint32_t brk = ~hc & from;
+                const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
+                const uint32_t tm = Tw & from & ((2u << e) - 1u);
+                const uint32_t key = tm ? sbase + 32 * q + (__ffs(tm) - 1) : sbase + TBW + 32 * q + s0;
+                const uint32_t x = rbase + 32 * q + s0;
+                P[x] = (key << 12) | x;
             }
         }
         __syncthreads();
-
-        // Phase B: the links to the row above, decided for the 8 blocks of a group at once on
-        // nibble-packed masks (bit 4k = block k), are queued in shared memory and then merged
-        // with every lane busy (one round per item, so the queue rarely overflows).
-#pragma unroll
-        for (int i = 0; i < ITEMS / K1_NT; ++i) {
-            const int it = tid + i * K1_NT, r = it / GROUPS, g = it % GROUPS;
-            const uint32_t ms = masks[i];
-            const int c0 = 8 * g;
-            uint32_t *qn = &mqn[i];
-            uint32_t hcl = 0, cN = 0, cNW = 0, cNE = 0, U = 0, UL = 0, UR = 0, ML = 0;
-            if (ms) {
-                ML = c0 > 0 ? M[r * TBW + c0 - 1] : 0u;
-                hcl = nb_lft(ms) & ((nb_rgt(ms) << 4) | nb_rgt(ML));
-                if (r > 0) {
-                    const uint8_t *Urow = &M[(r - 1) * TBW];
-                    const uint2 ub = *reinterpret_cast<const uint2 *>(Urow + c0);
-                    U = bytes_to_nibbles(ub.x) | (bytes_to_nibbles(ub.y) << 16);
-                    UL = c0 > 0 ? Urow[c0 - 1] : 0u;
-                    UR = c0 + 8 < TBW ? Urow[c0 + 8] : 0u;
-                    const uint32_t top = nb_b0(ms) | nb_b1(ms);
-                    const uint32_t uBL = nb_b2(U), uBR = nb_b3(U), uB = uBL | uBR;
-                    const uint32_t rawN = top & uB;
-                    cN = rawN;
-                    cNW = nb_b0(ms) & ((uBR << 4) | nb_b3(UL));
-                    cNE = nb_b1(ms) & ((uBL >> 4) | (nb_b2(UR) << 28));
-                    // Skip rules.  A link may be skipped when its two blocks are already joined
-                    // through links that are made or are themselves skipped for a reason further
-                    // left; every chain of reasons runs leftward along the run and ends at a
-                    // link that is made.
-                    // (1) The left block of the same run touches the same upper block.
-                    const uint32_t leftN = ((top << 4) | nb_b0(ML) | nb_b1(ML)) & ((uB << 4) | nb_b2(UL) | nb_b3(UL));
-                    const uint32_t leftNE = ((nb_b1(ms) << 4) | nb_b1(ML)) & uBL;
-                    cNW &= ~(hcl & leftN);
-                    cN &= ~(hcl & leftNE);
-                    // (2) The upper diagonal block is joined horizontally to the block straight
-                    //     above, which this block touches.
-                    const uint32_t uL = nb_lft(U), uR = nb_rgt(U);
-                    cNW &= ~(rawN & (((uR << 4) | nb_rgt(UL)) & uL));
-                    cNE &= ~(rawN & (uR & ((uL >> 4) | (nb_lft(UR) << 28))));
-                }
+        // A run that entered from the left and has a top pixel here may have a smaller slot.
+        if (cin) {
+            const uint32_t brk = ~hc;
+            const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
+            const uint32_t tm = Tw & ((2u << e) - 1u);
+            if (tm && GUARD(w, CSc < uint32_t(TBW), 111, CSc)) {
+                const uint32_t x = rbase + (CSc & (TBW - 1));
+                atomicMin(&P[x], ((sbase + 32 * q + (__ffs(tm) - 1)) << 12) | x);
             }
-            const uint32_t n = __popc(cN) + __popc(cNW) + __popc(cNE);
-            uint32_t pos = warp_reserve(qn, n);
+        }
+        __syncthreads();   // slots final before any union reads them
+
+        // Phase B: links to the block row above.  For block b of this row: N (straight up, a top
+        // pixel over a bottom pixel), NW (top-left pixel to the bottom-right pixel of b - 1 above)
+        // and NE (top-right to the bottom-left pixel of b + 1 above).  A link is dropped when an
+        // earlier link (further left, or N before NW / NE at the same block) joins the same two
+        // runs; every chain of such reasons ends at a link that is kept.
+        uint32_t Nm = 0, NWm = 0, NEm = 0, uS = 0, uCS = 0;
+        if (r > 0 && r < nbr) {
+            const int u = tid - WPR;   // same word, row above
+            const uint32_t uBL = WBL[u], uBR = WBR[u], uhc = WHC[u];
+            uS = WS[u];
+            uCS = WCS[u];
+            const uint32_t uBRp = q > 0 ? WBR[u - 1] >> 31 : 0u;
+            const uint32_t uBLn = q + 1 < WPR ? WBL[u + 1] & 1u : 0u;
+            const uint32_t uhl = (uhc << 1) | (q > 0 ? WHC[u - 1] >> 31 : 0u);
+            const uint32_t N = Tw & (uBL | uBR);
+            const uint32_t NW = TLw & ((uBR << 1) | uBRp);
+            const uint32_t NE = TRw & ((uBL >> 1) | (uBLn << 31));
+            Nm = N; NWm = NW; NEm = NE;
+        }
+        {
+            // bit 31 of the previous word's raw N / NE, for the rules at block 0
+            const uint32_t Np = __shfl_up_sync(0xFFFFFFFFu, Nm, 1, WPR);
+            const uint32_t NEp = __shfl_up_sync(0xFFFFFFFFu, NEm, 1, WPR);
+            if (r > 0 && r < nbr) {
+                const int u = tid - WPR;
+                const uint32_t uhc = WHC[u];
+                const uint32_t uhl = (uhc << 1) | (q > 0 ? WHC[u - 1] >> 31 : 0u);
+                const uint32_t N = Nm, NE = NEm;
+                const uint32_t Nsh = (N << 1) | (q > 0 ? Np >> 31 : 0u);
+                const uint32_t NEsh = (NE << 1) | (q > 0 ? NEp >> 31 : 0u);
+                Nm = N & ~(hl & ((Nsh & uhl) | NEsh));
+                NWm &= ~((N & uhl) | (hl & Nsh));
+                NEm = NE & ~((N & uhc) | (hl & NEsh & uhc));
+            }
+        }
+        const uint32_t n = __popc(Nm) + __popc(NWm) + __popc(NEm);
+        uint32_t pos = warp_reserve(&mqn, n);
+        {
+            const uint32_t ubase = rbase - TBW;
+            // Start column of the run holding block column c (in this word, c in [0, 31]) of a
+            // row with run starts S_ and carried start CS_.
+            auto start_in = [&](uint32_t S_, uint32_t CS_, uint32_t c) -> uint32_t {
+                const uint32_t m = S_ & ((2u << c) - 1u);
+                return m ? uint32_t(32 * q) + hibit(m) : CS_;
+            };
             auto push = [&](uint32_t a, uint32_t b) {
-                if (pos < MQCAP) MQ[pos] = (a << 16) | b;
-                else smerge(P, a, b);   // queue full: merge in place
+                // Both are run starts of this tile by construction; the mask only keeps a
+                // broken invariant from leaving the array.
+                GUARD(w, a < uint32_t(NBLK) && b < uint32_t(NBLK), 112, (uint64_t(a) << 32) | b);
+                a &= NBLK - 1;
+                b &= NBLK - 1;
+                if (pos < uint32_t(MQCAP)) MQ[pos] = (a << 16) | b;
+                else eunion(P, a, b);   // queue full: merge in place
                 ++pos;
             };
-            uint32_t todo = cN | cNW | cNE;
+            uint32_t todo = Nm | NWm | NEm;
             while (todo) {
-                const int k = (__ffs(todo) - 1) >> 2;
-                const uint32_t bit = 1u << (4 * k);
-                todo &= ~bit;
-                const int c = c0 + k;
-                const uint32_t sl = slot_of(r, c, (ms >> (4 * k)) & 15u);
-                if (cN & bit) push(sl, slot_of(r - 1, c, (U >> (4 * k)) & 15u));
-                if (cNW & bit) push(sl, slot_of(r - 1, c - 1, k ? (U >> (4 * k - 4)) & 15u : UL));
-                if (cNE & bit) push(sl, slot_of(r - 1, c + 1, k < 7 ? (U >> (4 * k + 4)) & 15u : UR));
-            }
-            __syncthreads();
-            const uint32_t nq = min(*qn, uint32_t(MQCAP));
-            for (uint32_t q = tid; q < nq; q += K1_NT) smerge(P, MQ[q] >> 16, MQ[q] & 0xFFFFu);
-            __syncthreads();
-        }
-
-        // Phase C: resolve each block's root (read-only: all merges are done), write tile-local
-        // labels, mark roots.
-#pragma unroll
-        for (int i = 0; i < ITEMS / K1_NT; ++i) {
-            const int it = tid + i * K1_NT, r = it / GROUPS, g = it % GROUPS;
-            const uint32_t ms = masks[i];
-            uint32_t e[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t m = (ms >> (4 * k)) & 15u;
-                e[k] = 0;
-                if (!m) continue;
-                const int c = 8 * g + k;
-                const uint32_t s = slot_of(r, c, m);
-                const uint32_t root = sflatten(P, s);
-                const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
-                e[k] = (m << 12) | rb;
-                if (root == s) {
-                    int dy, dx;
-                    first_px(m, dy, dx);
-                    const int y = 2 * r + dy, x = 2 * c + dx;
-                    atomicOr(&RB[y][x >> 5], 1u << (x & 31));
+                const uint32_t b = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const uint32_t bit = 1u << b;
+                const uint32_t a = rbase + start_in(S, CSc, b);
+                if (Nm & bit) push(a, ubase + start_in(uS, uCS, b));
+                if (NWm & bit) {
+                    uint32_t c;
+                    if (b > 0) c = start_in(uS, uCS, b - 1);
+                    else {
+                        const uint32_t pS = WS[tid - WPR - 1];
+                        c = pS ? uint32_t(32 * (q - 1)) + hibit(pS) : WCS[tid - WPR - 1];
+                    }
+                    push(a, ubase + c);
+                }
+                if (NEm & bit) {
+                    uint32_t c;
+                    if (b < 31) c = start_in(uS, uCS, b + 1);
+                    else c = (WS[tid - WPR + 1] & 1u) ? uint32_t(32 * (q + 1)) : WCS[tid - WPR + 1];
+                    push(a, ubase + c);
                 }
             }
-            uint4 v;
-            v.x = e[0] | (e[1] << 16); v.y = e[2] | (e[3] << 16);
-            v.z = e[4] | (e[5] << 16); v.w = e[6] | (e[7] << 16);
-            *reinterpret_cast<uint4 *>(lab + t * NBLK + r * TBW + 8 * g) = v;
         }
         __syncthreads();
+        {
+            const uint32_t nq = min(mqn, uint32_t(MQCAP));
+            for (uint32_t i = tid; i < nq; i += K1_NT) eunion(P, MQ[i] >> 16, MQ[i] & 0xFFFFu);
+        }
+        __syncthreads();
+
+        // Phase C: every run start points straight at its root; roots mark their first pixel.
+        {
+            uint32_t ss = S;
+            while (ss) {
+                const uint32_t s0 = __ffs(ss) - 1;
+                ss &= ss - 1;
+                const uint32_t x = rbase + 32 * q + s0;
+                const uint32_t root = efind_ro(P, x);
+                const uint32_t ev = P[root];
+                // Point the whole path at the root (every writer stores the same final value), so
+                // the long chains of thin vertical lines are walked once.
+                for (uint32_t y = x; y != root;) {
+                    const uint32_t ny = P[y] & 0xFFFu;
+                    P[y] = ev;
+                    y = ny;
+                }
+                if (root == x) {
+                    const uint32_t key = ev >> 12;
+                    const uint32_t rb = key_block(key);
+                    int dy, dx;
+                    first_px(M[rb], dy, dx);
+                    const int y = 2 * int(key / (2 * TBW)) + dy, xx = 2 * int(key % TBW) + dx;
+                    atomicOr(&RB[y][xx >> 5], 1u << (xx & 31));
+                }
+            }
+        }
+        __syncthreads();
+        // Block entries (mask << 12) | root block, two blocks per 32-bit word.
+        {
+            uint32_t cur = cin ? key_block(P[rbase + (CSc & (TBW - 1))] >> 12) : 0u;
+            uint32_t ew[16];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                if ((S >> k) & 1u) cur = key_block(P[rbase + 32 * q + k] >> 12);
+                const uint32_t m = (mw[k >> 2] >> (8 * (k & 3))) & 15u;
+                const uint32_t e = m ? (m << 12) | cur : 0u;
+                if (k & 1) ew[k >> 1] |= e << 16;
+                else ew[k >> 1] = e;
+            }
+            uint4 *dst = reinterpret_cast<uint4 *>(lab + t * NBLK + rbase + 32 * q);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) dst[i] = make_uint4(ew[4 * i], ew[4 * i + 1], ew[4 * i + 2], ew[4 * i + 3]);
+        }
 
         // Phase D: root bitmap and segment counts out; border components -> nodes.
         for (int i = tid; i < TH * (TW / 32); i += K1_NT) w.rbits[t * (TH * (TW / 32)) + i] = (&RB[0][0])[i];
@@ -301,20 +403,23 @@ __global__ void __launch_bounds__(K1_NT, 4) k_tile_local_2d(ImgList2D L, Work w)
 #pragma unroll
         for (int i = 0; i < (NPERIM + K1_NT - 1) / K1_NT; ++i) {
             const int p = tid + i * K1_NT;
-            int r, c;
+            int br, bc;
             prb[i] = kNone;
-            if (p >= NPERIM || !perim_pos(p, nbr, nbc, r, c)) continue;
-            const uint32_t m = M[r * TBW + c];
+            if (p >= NPERIM || !perim_pos(p, nbr, nbc, br, bc)) continue;
+            const uint32_t m = M[br * TBW + bc];
             if (!m) continue;
-            const uint32_t root = sfind_ro(P, slot_of(r, c, m));
-            const uint32_t rb = (root / (2 * TBW)) * TBW + (root % TBW);
+            const int wi = br * WPR + (bc >> 5);
+            const uint32_t sm = WS[wi] & ((2u << (bc & 31)) - 1u);
+            const uint32_t sc = sm ? uint32_t(bc & ~31) + hibit(sm) : WCS[wi];
+            GUARD(w, sc < uint32_t(TBW), 113, sc);
+            const uint32_t rb = key_block(P[uint32_t(br) * TBW + (sc & (TBW - 1))] >> 12);
             prb[i] = rb | (m << 16);
             atomicOr(&BF[rb >> 5], 1u << (rb & 31));
         }
         __syncthreads();
         uint32_t nb;
-        const uint32_t pre = block_exscan<K1_NT>(tid < NBLK / 32 ? __popc(BF[tid]) : 0u, tmp, &nb);
-        if (tid < NBLK / 32) BP[tid] = pre;
+        const uint32_t pre = block_exscan<K1_NT>(__popc(BF[tid]), tmp, &nb);
+        BP[tid] = pre;
         __syncthreads();
         // Every border position writes its entry and (redundantly, with identical values) the
         // record of the node its root belongs to, which spreads the node work over the CTA.
@@ -656,7 +761,7 @@ inline cudaError_t launch(const ImgList2D &L, const Work &w, int sms, bool persi
     Work wk = w;
     if (!persistent) wk.queue = nullptr;
     mark(0);
-    k_tile_local_2d<<<grid(w.n_tiles, 4), K1_NT, 0, s>>>(L, wk);
+    k_tile_local_2d<<<grid(w.n_tiles, 5), K1_NT, 0, s>>>(L, wk);
     mark(1);
     k_merge_2d<<<grid(w.n_tiles, 8), K2_NT, 0, s>>>(L, wk);
     mark(2);
