@@ -488,78 +488,161 @@ __device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
 
 }  // namespace
 
-// Cross-tile pairs go through a CTA-local node filter (be_common.cuh: NodeFilter) and only the
-// pairs that join two local sets are unioned globally, from a shared queue after all pairs of
-// the tile are seen; dense volumes produce the same few border components from hundreds of face
-// blocks.
-constexpr int kFilterSlots3 = 4096;
+// Cross-tile merge over the +d0, +d1 and +d2 faces.  The border entries of the blocks across
+// each + face (the next tile's - face, widened by one block on every side into the diagonal
+// tiles) are staged in shared memory once per tile, so each face block checks its nine
+// neighbours without index arithmetic or global loads.  A CTA-local union-find over this tile's
+// nodes and the staged positions then filters the pairs: only a pair that joins two local sets
+// goes on to the global union-find (from a shared queue, once the tile's pairs are all seen); a
+// dense volume that crosses a face with one component in hundreds of blocks costs a handful of
+// global unions.
 constexpr int kGQ3 = 1024;   // queued global unions per tile (more are done at once)
+constexpr int PF0 = (TB1 + 2) * (TB2 + 2);   // staged entries across the +d0 face
+constexpr int PF1 = (TB0 + 2) * (TB2 + 2);   // +d1
+constexpr int PF2 = (TB0 + 2) * (TB1 + 2);   // +d2
+constexpr int NPF = PF0 + PF1 + PF2;
+constexpr int NPLUS = TB1 * TB2 + TB0 * TB2 + TB0 * TB1;
+
+// Face geometry along axis AX (compile-time, so nothing is indexed at run time): the two tangent
+// axes in order, their tile sizes, the staged array's offset and pitch.
+template <int AX> struct FaceAx {
+    static constexpr int A1 = AX == 0 ? 1 : 0, A2 = AX == 2 ? 1 : 2;
+    static constexpr int TA = A1 == 0 ? TB0 : TB1, TBb = A2 == 1 ? TB1 : TB2;
+    static constexpr int TAX = AX == 0 ? TB0 : AX == 1 ? TB1 : TB2;
+    static constexpr int EBASE = AX == 0 ? 0 : AX == 1 ? PF0 : PF0 + PF1;
+    static constexpr int PITCH = TBb + 2;
+    static constexpr int NPOS = TA * TBb;
+    static constexpr int PBASE = AX == 0 ? 0 : AX == 1 ? TB1 * TB2 : TB1 * TB2 + TB0 * TB2;
+};
+
+__device__ __forceinline__ int pick3(int a0, int a1, int a2, int i) { return i == 0 ? a0 : i == 1 ? a1 : a2; }
+
+// Stage entry e (0 <= e < (TA+2) * (TBb+2)) of the face along AX.
+template <int AX>
+__device__ __forceinline__ void stage_face(const Img3D &im, const TileGeo &g, Work &w, int e, uint32_t *nbid,
+                                           uint8_t *nbf)
+{
+    using F = FaceAx<AX>;
+    const int iu = e / F::PITCH, iv = e % F::PITCH;
+    const int tcx = pick3(g.tx0, g.tx1, g.tx2, AX), tnx = pick3(im.t0, im.t1, im.t2, AX);
+    const int tc1 = pick3(g.tx0, g.tx1, g.tx2, F::A1), tc2 = pick3(g.tx0, g.tx1, g.tx2, F::A2);
+    const int nb1 = (pick3(im.d0, im.d1, im.d2, F::A1) + 1) >> 1, nb2 = (pick3(im.d0, im.d1, im.d2, F::A2) + 1) >> 1;
+    const int g1 = tc1 * F::TA + iu - 1, g2 = tc2 * F::TBb + iv - 1;
+    uint32_t id = kNone, fb = 0;
+    if (tcx + 1 < tnx && g1 >= 0 && g1 < nb1 && g2 >= 0 && g2 < nb2) {
+        const int t1 = g1 / F::TA, l1 = g1 - t1 * F::TA, t2 = g2 / F::TBb, l2 = g2 - t2 * F::TBb;
+        int tt0, tt1, tt2;
+        if (AX == 0) { tt0 = tcx + 1; tt1 = t1; tt2 = t2; }
+        else if (AX == 1) { tt0 = t1; tt1 = tcx + 1; tt2 = t2; }
+        else { tt0 = t1; tt1 = t2; tt2 = tcx + 1; }
+        const int64_t t2i = im.tile_base + (int64_t(tt0) * im.t1 + tt1) * im.t2 + tt2;
+        const int qb = l1 * F::TBb + l2;   // position on the - face: (first tangent, second tangent)
+        if (GUARD(w, t2i >= 0 && t2i < w.n_tiles && qb >= 0 && qb < NPERIM, 201, t2i)) {
+            const uint32_t B = w.perim[t2i * NPERIM + face_base(2 * AX) + qb];
+            if (B && GUARD(w, (B >> 4) < w.nb[t2i], 203, (uint64_t(t2i) << 16) | (B >> 4))) {
+                id = uint32_t(t2i * MAXB + (B >> 4));
+                fb = B & 15u;
+            }
+        }
+    }
+    nbid[F::EBASE + e] = id;
+    nbf[F::EBASE + e] = uint8_t(fb);
+}
+
+// This tile's + face entry at position q of the face along AX (0 when the face has no neighbour).
+template <int AX>
+__device__ __forceinline__ uint32_t plus_entry(const Img3D &im, const TileGeo &g, const Work &w, int64_t t, int q,
+                                               int &u, int &v)
+{
+    using F = FaceAx<AX>;
+    u = q / F::TBb;
+    v = q % F::TBb;
+    const int tcx = pick3(g.tx0, g.tx1, g.tx2, AX), tnx = pick3(im.t0, im.t1, im.t2, AX);
+    const int n1 = pick3(g.n0, g.n1, g.n2, F::A1), n2 = pick3(g.n0, g.n1, g.n2, F::A2);
+    if (tcx + 1 >= tnx || u >= n1 || v >= n2) return 0u;
+    return w.perim[t * NPERIM + face_base(2 * AX + 1) + q];
+}
+
+// Staged position e of the face along AX -> (iu, iv) in the staged grid, or false when e lies in
+// another face's range.
+template <int AX>
+__device__ __forceinline__ bool staged_pos(int e, int &iu, int &iv)
+{
+    using F = FaceAx<AX>;
+    const int k = e - F::EBASE;
+    if (k < 0 || k >= (F::TA + 2) * F::PITCH) return false;
+    iu = k / F::PITCH;
+    iv = k % F::PITCH;
+    return true;
+}
 
 __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Work w)
 {
     __shared__ uint32_t qslot;
-    __shared__ NodeFilter<kFilterSlots3> flt;
+    __shared__ uint32_t lp[MAXB + NPF];   // local union-find: this tile's nodes, then staged positions
+    __shared__ uint32_t nbid[NPF];        // global node id across the face, kNone = none
+    __shared__ uint8_t nbf[NPF];          // its face bits
     __shared__ uint2 gq[kGQ3];
-    constexpr int NPLUS = TB1 * TB2 + TB0 * TB2 + TB0 * TB1;
+    __shared__ uint32_t nq;
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
         const Img3D im = L.get(t);
         const TileGeo g = tile_geo(im, t);
-        const int nbk[3] = {(im.d0 + 1) >> 1, (im.d1 + 1) >> 1, (im.d2 + 1) >> 1};
-        const int tb[3] = {TB0, TB1, TB2};
-        const int tc[3] = {g.tx0, g.tx1, g.tx2};
-        const int tn[3] = {im.t0, im.t1, im.t2};
-        filter_reset(flt);
+        for (int i = threadIdx.x; i < MAXB + NPF; i += kT3MergeThreads) lp[i] = uint32_t(i);
+        if (threadIdx.x == 0) nq = 0;
+        for (int e = threadIdx.x; e < PF0; e += kT3MergeThreads) stage_face<0>(im, g, w, e, nbid, nbf);
+        for (int e = threadIdx.x; e < PF1; e += kT3MergeThreads) stage_face<1>(im, g, w, e, nbid, nbf);
+        for (int e = threadIdx.x; e < PF2; e += kT3MergeThreads) stage_face<2>(im, g, w, e, nbid, nbf);
         __syncthreads();
+        // Staged positions of the same node that touch on the face are one element from here on
+        // (a component crosses a face as a patch, not as scattered blocks).
+        for (int e = threadIdx.x; e < NPF; e += kT3MergeThreads) {
+            const uint32_t id = nbid[e];
+            if (id == kNone) continue;
+            int iu, iv, pitch;
+            if (staged_pos<0>(e, iu, iv)) pitch = FaceAx<0>::PITCH;
+            else if (staged_pos<1>(e, iu, iv)) pitch = FaceAx<1>::PITCH;
+            else { staged_pos<2>(e, iu, iv); pitch = FaceAx<2>::PITCH; }
+            if (iv > 0 && nbid[e - 1] == id) smerge(lp, uint32_t(MAXB + e), uint32_t(MAXB + e - 1));
+            if (iu > 0 && nbid[e - pitch] == id) smerge(lp, uint32_t(MAXB + e), uint32_t(MAXB + e - pitch));
+        }
+        __syncthreads();
+        // Pairs: a pair whose two elements are already one local set is implied by pairs queued
+        // before it (smerge_joined); the rest are unioned globally after the loop.
         for (int p = threadIdx.x; p < NPLUS; p += kT3MergeThreads) {
-            int axis, q;
-            if (p < TB1 * TB2) { axis = 0; q = p; }
-            else if (p < TB1 * TB2 + TB0 * TB2) { axis = 1; q = p - TB1 * TB2; }
-            else { axis = 2; q = p - TB1 * TB2 - TB0 * TB2; }
-            if (tc[axis] + 1 >= tn[axis]) continue;
-            const int f = 2 * axis + 1;
-            int lb[3];
-            if (axis == 0) { lb[0] = g.n0 - 1; lb[1] = q / TB2; lb[2] = q % TB2; }
-            else if (axis == 1) { lb[1] = g.n1 - 1; lb[0] = q / TB2; lb[2] = q % TB2; }
-            else { lb[2] = g.n2 - 1; lb[0] = q / TB1; lb[1] = q % TB1; }
-            if (lb[0] >= g.n0 || lb[1] >= g.n1 || lb[2] >= g.n2) continue;
-            const uint32_t A = w.perim[t * NPERIM + face_base(f) + q];
-            if (!A) continue;
-            const uint32_t fa = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
-            if (!GUARD(w, (A >> 4) < w.nb[t], 204, (uint64_t(t) << 16) | (A >> 4))) continue;
-            const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;   // tangent axes in order
-            uint32_t last = kNone;
+            int u = 0, v = 0, ebase, pitch;
+            uint32_t A;
+            if (p < FaceAx<0>::NPOS) {
+                A = plus_entry<0>(im, g, w, t, p, u, v);
+                ebase = FaceAx<0>::EBASE; pitch = FaceAx<0>::PITCH;
+            } else if (p < FaceAx<0>::NPOS + FaceAx<1>::NPOS) {
+                A = plus_entry<1>(im, g, w, t, p - FaceAx<1>::PBASE, u, v);
+                ebase = FaceAx<1>::EBASE; pitch = FaceAx<1>::PITCH;
+            } else {
+                A = plus_entry<2>(im, g, w, t, p - FaceAx<2>::PBASE, u, v);
+                ebase = FaceAx<2>::EBASE; pitch = FaceAx<2>::PITCH;
+            }
+            if (!A || !GUARD(w, (A >> 4) < w.nb[t] && (A >> 4) < uint32_t(MAXB), 204, (uint64_t(t) << 16) | (A >> 4)))
+                continue;
+            const uint32_t fa = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
+#pragma unroll
             for (int da = -1; da <= 1; ++da) {
+#pragma unroll
                 for (int db = -1; db <= 1; ++db) {
                     if (!(fa & face_sel(da, db))) continue;
-                    int gbk[3];
-                    gbk[axis] = tc[axis] * tb[axis] + lb[axis] + 1;
-                    gbk[ax1] = tc[ax1] * tb[ax1] + lb[ax1] + da;
-                    gbk[ax2] = tc[ax2] * tb[ax2] + lb[ax2] + db;
-                    if (gbk[ax1] < 0 || gbk[ax1] >= nbk[ax1] || gbk[ax2] < 0 || gbk[ax2] >= nbk[ax2]) continue;
-                    int tt[3], lc[3];
-                    for (int a = 0; a < 3; ++a) { tt[a] = gbk[a] / tb[a]; lc[a] = gbk[a] - tt[a] * tb[a]; }
-                    const int64_t t2i = im.tile_base + (int64_t(tt[0]) * im.t1 + tt[1]) * im.t2 + tt[2];
-                    const int qb = axis == 0 ? lc[1] * TB2 + lc[2] : axis == 1 ? lc[0] * TB2 + lc[2]
-                                                                              : lc[0] * TB1 + lc[1];
-                    if (!GUARD(w, t2i >= 0 && t2i < w.n_tiles && qb >= 0 && qb < NPERIM, 201, t2i)) continue;
-                    const uint32_t B = w.perim[t2i * NPERIM + face_base(2 * axis) + qb];
-                    if (!B) continue;
-                    if (!((B & 15u) & face_sel(-da, -db))) continue;
-                    const uint32_t nB = uint32_t(t2i * MAXB + (B >> 4));
-                    if (!GUARD(w, (B >> 4) < w.nb[t2i], 203, (uint64_t(t2i) << 16) | (B >> 4))) continue;
-                    if (nB == last) continue;
-                    last = nB;
-                    if (!filter_pair(flt, nA, nB)) continue;
-                    const uint32_t slot = atomicAdd(&flt.nq, 1u);
-                    if (slot < uint32_t(kGQ3)) gq[slot] = make_uint2(nA, nB);
-                    else gunion3d(im, w, nA, nB);
+                    const int e = ebase + (u + 1 + da) * pitch + (v + 1 + db);
+                    const uint32_t id = nbid[e];
+                    if (id == kNone || !(nbf[e] & face_sel(-da, -db))) continue;
+                    if (!smerge_joined(lp, ja, uint32_t(MAXB + e))) continue;
+                    const uint32_t slot = atomicAdd(&nq, 1u);
+                    if (slot < uint32_t(kGQ3)) gq[slot] = make_uint2(nA, id);
+                    else gunion3d(im, w, nA, id);
                 }
             }
         }
         __syncthreads();
-        const uint32_t nq = min(flt.nq, uint32_t(kGQ3));
-        for (uint32_t i = threadIdx.x; i < nq; i += kT3MergeThreads) gunion3d(im, w, gq[i].x, gq[i].y);
+        const uint32_t nqt = min(nq, uint32_t(kGQ3));
+        for (uint32_t i = threadIdx.x; i < nqt; i += kT3MergeThreads) gunion3d(im, w, gq[i].x, gq[i].y);
         __syncthreads();
     }
 }
