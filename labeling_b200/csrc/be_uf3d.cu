@@ -502,6 +502,7 @@ constexpr int PF1 = (TB0 + 2) * (TB2 + 2);   // +d1
 constexpr int PF2 = (TB0 + 2) * (TB1 + 2);   // +d2
 constexpr int NPF = PF0 + PF1 + PF2;
 constexpr int NPLUS = TB1 * TB2 + TB0 * TB2 + TB0 * TB1;
+constexpr int NSROWS = (TB1 + 2) + (TB0 + 2) + (TB0 + 2);   // staged rows over the three faces
 
 // Face geometry along axis AX (compile-time, so nothing is indexed at run time): the two tangent
 // axes in order, their tile sizes, the staged array's offset and pitch.
@@ -595,7 +596,26 @@ __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Wo
         for (int e = threadIdx.x; e < PF2; e += kT3MergeThreads) stage_face<2>(im, g, w, e, nbid, nbf);
         __syncthreads();
         // Staged positions of the same node that touch on the face are one element from here on
-        // (a component crosses a face as a patch, not as scattered blocks).
+        // (a component crosses a face as a patch, not as scattered blocks): runs along each staged
+        // row point at their first position, runs of neighbouring rows are merged where one of
+        // them starts, and every staged position is then pointed straight at its root.
+        for (int row = threadIdx.x; row < NSROWS; row += kT3MergeThreads) {
+            int e0, n;
+            if (row < FaceAx<0>::TA + 2) { e0 = FaceAx<0>::EBASE + row * FaceAx<0>::PITCH; n = FaceAx<0>::PITCH; }
+            else if (row < FaceAx<0>::TA + FaceAx<1>::TA + 4) {
+                e0 = FaceAx<1>::EBASE + (row - FaceAx<0>::TA - 2) * FaceAx<1>::PITCH; n = FaceAx<1>::PITCH;
+            } else {
+                e0 = FaceAx<2>::EBASE + (row - FaceAx<0>::TA - FaceAx<1>::TA - 4) * FaceAx<2>::PITCH; n = FaceAx<2>::PITCH;
+            }
+            uint32_t prev = kNone, start = 0;
+            for (int k = 0; k < n; ++k) {
+                const uint32_t id = nbid[e0 + k];
+                if (id != prev) start = uint32_t(MAXB + e0 + k);
+                lp[MAXB + e0 + k] = start;
+                prev = id;
+            }
+        }
+        __syncthreads();
         for (int e = threadIdx.x; e < NPF; e += kT3MergeThreads) {
             const uint32_t id = nbid[e];
             if (id == kNone) continue;
@@ -603,9 +623,15 @@ __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Wo
             if (staged_pos<0>(e, iu, iv)) pitch = FaceAx<0>::PITCH;
             else if (staged_pos<1>(e, iu, iv)) pitch = FaceAx<1>::PITCH;
             else { staged_pos<2>(e, iu, iv); pitch = FaceAx<2>::PITCH; }
-            if (iv > 0 && nbid[e - 1] == id) smerge(lp, uint32_t(MAXB + e), uint32_t(MAXB + e - 1));
-            if (iu > 0 && nbid[e - pitch] == id) smerge(lp, uint32_t(MAXB + e), uint32_t(MAXB + e - pitch));
+            if (iu == 0 || nbid[e - pitch] != id) continue;
+            // One link per pair of overlapping runs: at the overlap's first column, where one of
+            // the two runs starts.
+            const bool xs = iv == 0 || nbid[e - 1] != id, ys = iv == 0 || nbid[e - pitch - 1] != id;
+            if (xs || ys) smerge(lp, uint32_t(MAXB + e), uint32_t(MAXB + e - pitch));
         }
+        __syncthreads();
+        for (int e = threadIdx.x; e < NPF; e += kT3MergeThreads)
+            if (nbid[e] != kNone) sflatten(lp, uint32_t(MAXB + e));
         __syncthreads();
         // Pairs: a pair whose two elements are already one local set is implied by pairs queued
         // before it (smerge_joined); the rest are unioned globally after the loop.
