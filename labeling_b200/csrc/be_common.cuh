@@ -312,42 +312,13 @@ __device__ __forceinline__ uint32_t gfind_ro(const uint32_t *gp, uint32_t a)
     return a;
 }
 
-// ---- Border-merge filter: a CTA-local union-find over global node ids ----------------------
+// ---- Border-merge filter ---------------------------------------------------------------------
 // The cross-tile merge kernels see the same pair of border components over and over (every face
 // position of a large component yields one).  Before a pair costs a global union (dependent loads
-// through L2), it is merged in a small shared-memory union-find keyed by node id: only a pair that
-// joins two different local sets goes on to the global union-find; a pair already connected by
-// earlier local merges is implied by the global unions those merges queued.
-template <int KH>
-struct NodeFilter {
-    uint32_t key[KH];    // node id per slot, kNone = empty
-    uint32_t par[KH];    // local union-find parent per slot
-    uint32_t nq;         // queued global unions
-};
-
-template <int KH>
-__device__ __forceinline__ void filter_reset(NodeFilter<KH> &f)
-{
-    for (int i = threadIdx.x; i < KH; i += blockDim.x) {
-        f.key[i] = kNone;
-        f.par[i] = uint32_t(i);
-    }
-    if (threadIdx.x == 0) f.nq = 0;
-}
-
-// Slot of node id `n` (inserted when new), or -1 when the probe sequence is full.
-template <int KH>
-__device__ __forceinline__ int filter_slot(NodeFilter<KH> &f, uint32_t n)
-{
-    uint32_t h = (n * 2654435761u) & uint32_t(KH - 1);
-    for (int probe = 0; probe < 32; ++probe) {
-        const uint32_t old = atomicCAS(&f.key[h], kNone, n);
-        if (old == kNone || old == n) return int(h);
-        h = (h + 1) & uint32_t(KH - 1);
-    }
-    return -1;
-}
-
+// through L2), it is merged in a small shared-memory union-find over the tile's nodes and the
+// staged neighbour positions: only a pair that joins two different local sets goes on to the
+// global union-find; a pair already connected by earlier local merges is implied by the global
+// unions those merges queued.
 // Local merge of the sets of slots a and b (smaller slot wins, as smerge); false only when the
 // two were already one set and this call changed no parent.  An atomicMin that lands on an entry
 // another thread has just linked still rewrites that entry's parent (it moves the entry's subtree
@@ -372,15 +343,6 @@ __device__ __forceinline__ bool smerge_joined(uint32_t *P, uint32_t a, uint32_t 
             a = old;
         }
     }
-}
-
-// True when the pair (na, nb) must be unioned globally.
-template <int KH>
-__device__ __forceinline__ bool filter_pair(NodeFilter<KH> &f, uint32_t na, uint32_t nb)
-{
-    const int sa = filter_slot(f, na), sb = filter_slot(f, nb);
-    if (sa < 0 || sb < 0) return true;
-    return smerge_joined(f.par, uint32_t(sa), uint32_t(sb));
 }
 
 // Decrement a uint8 counter packed in a 32-bit word (the counter is >= 1 when this is called).

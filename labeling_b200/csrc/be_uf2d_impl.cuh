@@ -483,17 +483,26 @@ __device__ void gunion2d(const Img2D &im, Work &w, uint32_t a, uint32_t b)
 }  // namespace
 
 constexpr int K2_NT = TBH + TBW;
-constexpr int kFilterSlots2 = 2048;
-constexpr int kGQ2 = 512;   // queued global unions per tile (more are done at once)
+constexpr int kGQ2 = 512;                      // queued global unions per tile (more are done at once)
+constexpr int SR = MAXB;                       // local index of the staged right column
+constexpr int SD = MAXB + TBH;                 // local index of the staged bottom row (column -1 first)
+constexpr int NLOC2 = MAXB + TBH + TBW + 2;    // local union-find size
 
-// One thread per right-border and bottom-border position.  Every connected pair goes through the
-// CTA-local node filter (NodeFilter, be_common.cuh); the pairs that join two local sets are
-// unioned globally from a shared queue once the tile's pairs are all seen.
+// One thread per right-border and bottom-border position.  The border entries across the right
+// border (the next tile's left column) and the bottom border (the top row of the tile below,
+// widened by one block into the two diagonal tiles) are staged in shared memory with the global
+// node id they belong to.  A CTA-local union-find over this tile's nodes and the staged positions
+// (neighbouring staged positions of one node merged first) filters the pairs: only a pair that
+// joins two local sets goes on to the global union-find, from a shared queue once all of the
+// tile's pairs are seen.
 __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
 {
     __shared__ uint32_t qslot;
-    __shared__ NodeFilter<kFilterSlots2> flt;
+    __shared__ uint32_t lp[NLOC2];
+    __shared__ uint32_t sid[TBH + TBW + 2];   // staged global node ids (kNone = none)
+    __shared__ uint8_t smk[TBH + TBW + 2];    // staged masks
     __shared__ uint2 gq[kGQ2];
+    __shared__ uint32_t nq;
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
         const Img2D im = L.get(t);
@@ -503,11 +512,52 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
         const int nbc = (min(TW, im.cols - tx * TW) + 1) >> 1;
         const int p = threadIdx.x;
         const uint16_t *pe = w.perim;
-        filter_reset(flt);
+        for (int i = p; i < NLOC2; i += K2_NT) lp[i] = uint32_t(i);
+        if (p == 0) nq = 0;
+        // Stage: thread p < TBH takes right-column row p; the others take bottom-row column
+        // p - TBH, and the first of them also columns -1 and nbc.
+        {
+            auto stage = [&](int k, int64_t t2, int pos) {
+                const uint32_t B = pe[t2 * NPERIM + pos];
+                sid[k] = B ? uint32_t(t2 * MAXB + (B >> 4)) : kNone;
+                smk[k] = uint8_t(B & 15u);
+            };
+            if (p < TBH) {
+                if (p < nbr && tx + 1 < im.tiles_x) stage(p, t + 1, 2 * TBW + p);
+                else { sid[p] = kNone; smk[p] = 0; }
+            } else {
+                const int c = p - TBH;
+                const int k = TBH + 1 + c;
+                if (c < nbc && ty + 1 < im.tiles_y) stage(k, t + im.tiles_x, c);
+                else { sid[k] = kNone; smk[k] = 0; }
+                if (c == 0) {
+                    if (tx > 0 && ty + 1 < im.tiles_y) stage(TBH, t + im.tiles_x - 1, TBW - 1);
+                    else { sid[TBH] = kNone; smk[TBH] = 0; }
+                }
+                if (c == 1) {
+                    // column TBW: block 0 of the tile below-right (a tile with a right neighbour is
+                    // full-width; a narrower tile's column nbc is staged empty by its own thread)
+                    if (nbc == TBW && tx + 1 < im.tiles_x && ty + 1 < im.tiles_y)
+                        stage(TBH + TBW + 1, t + im.tiles_x + 1, 0);
+                    else { sid[TBH + TBW + 1] = kNone; smk[TBH + TBW + 1] = 0; }
+                }
+            }
+        }
         __syncthreads();
-        auto pair = [&](uint32_t nA, uint32_t nB) {
-            if (!filter_pair(flt, nA, nB)) return;
-            const uint32_t slot = atomicAdd(&flt.nq, 1u);
+        // Neighbouring staged positions of one node are one element.
+        if (p < TBH) {
+            if (p > 0 && sid[p] != kNone && sid[p] == sid[p - 1]) smerge(lp, uint32_t(SR + p), uint32_t(SR + p - 1));
+        } else {
+            const int k = p - TBH + 1;   // staged bottom index, column k - 1
+            if (sid[TBH + k] != kNone && sid[TBH + k] == sid[TBH + k - 1])
+                smerge(lp, uint32_t(SD + k), uint32_t(SD + k - 1));
+            if (p == TBH && sid[TBH + TBW + 1] != kNone && sid[TBH + TBW + 1] == sid[TBH + TBW])
+                smerge(lp, uint32_t(SD + TBW + 1), uint32_t(SD + TBW));
+        }
+        __syncthreads();
+        auto pair = [&](uint32_t ja, uint32_t nA, uint32_t le, uint32_t nB) {
+            if (!smerge_joined(lp, ja, le)) return;
+            const uint32_t slot = atomicAdd(&nq, 1u);
             if (slot < uint32_t(kGQ2)) gq[slot] = make_uint2(nA, nB);
             else gunion2d(im, w, nA, nB);
         };
@@ -516,21 +566,17 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
             const int r = p;
             const uint32_t A = (r < nbr && tx + 1 < im.tiles_x) ? pe[t * NPERIM + 2 * TBW + TBH + r] : 0u;
             if (A) {
-                const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
-                const int64_t t2 = t + 1;
-                uint32_t last = kNone;
+                const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
 #pragma unroll
                 for (int d = -1; d <= 1; ++d) {
                     const int rr = r + d;
                     if (rr < 0 || rr >= nbr) continue;
-                    const uint32_t B = pe[t2 * NPERIM + 2 * TBW + rr];
-                    if (!B) continue;
-                    const uint32_t mB = B & 15u;
+                    const uint32_t nB = sid[rr];
+                    if (nB == kNone) continue;
+                    const uint32_t mB = smk[rr];
                     const bool c = d == 0 ? ((mA & 0xAu) && (mB & 0x5u))
                                           : d < 0 ? ((mA & 2u) && (mB & 4u)) : ((mA & 8u) && (mB & 1u));
-                    const uint32_t nB = uint32_t(t2 * MAXB + (B >> 4));
-                    if (c && nB != last) pair(nA, nB);
-                    if (c) last = nB;
+                    if (c) pair(ja, nA, uint32_t(SR + rr), nB);
                 }
             }
         } else {
@@ -538,35 +584,22 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
             const int c = p - TBH;
             const uint32_t A = (c < nbc && ty + 1 < im.tiles_y) ? pe[t * NPERIM + TBW + c] : 0u;
             if (A) {
-                const uint32_t mA = A & 15u, nA = uint32_t(t * MAXB + (A >> 4));
-                uint32_t last = kNone;
+                const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
 #pragma unroll
                 for (int d = -1; d <= 1; ++d) {
-                    int cc = c + d;
-                    int64_t t2 = t + im.tiles_x;
-                    if (cc < 0) {
-                        if (tx == 0) continue;
-                        t2 -= 1;
-                        cc = TBW - 1;
-                    } else if (cc >= nbc) {
-                        if (tx + 1 >= im.tiles_x) continue;
-                        t2 += 1;
-                        cc = 0;
-                    }
-                    const uint32_t B = pe[t2 * NPERIM + cc];
-                    if (!B) continue;
-                    const uint32_t mB = B & 15u;
+                    const int k = c + d + 1;   // staged bottom index
+                    const uint32_t nB = sid[TBH + k];
+                    if (nB == kNone) continue;
+                    const uint32_t mB = smk[TBH + k];
                     const bool cn = d == 0 ? ((mA & 0xCu) && (mB & 0x3u))
                                            : d < 0 ? ((mA & 4u) && (mB & 2u)) : ((mA & 8u) && (mB & 1u));
-                    const uint32_t nB = uint32_t(t2 * MAXB + (B >> 4));
-                    if (cn && nB != last) pair(nA, nB);
-                    if (cn) last = nB;
+                    if (cn) pair(ja, nA, uint32_t(SD + k), nB);
                 }
             }
         }
         __syncthreads();
-        const uint32_t nq = min(flt.nq, uint32_t(kGQ2));
-        for (uint32_t i = threadIdx.x; i < nq; i += K2_NT) gunion2d(im, w, gq[i].x, gq[i].y);
+        const uint32_t nqt = min(nq, uint32_t(kGQ2));
+        for (uint32_t i = threadIdx.x; i < nqt; i += K2_NT) gunion2d(im, w, gq[i].x, gq[i].y);
         __syncthreads();
     }
 }
