@@ -32,6 +32,8 @@ import time
 
 import numpy as np
 
+from labeling_b200 import replicas
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -225,7 +227,7 @@ def bench_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     is3d = args.workload == "3d512"
     if is3d:
-        inputs = make_3d_inputs(512, seed=100 + 17 * rank, only=args.families)
+        inputs = make_3d_inputs(512, seed=replicas.replica_seed(100, rank), only=args.families)
         stages = STAGES_3D
         metric, unit = "Gvox/s labeled (3D 512^3 BE, 26-conn)", "Gvox/s"
     else:
@@ -234,7 +236,7 @@ def bench_ours(args, rank, world, local_rank):
         if args.families:
             fams = args.families.split(",")
         from labeling_b200 import workloads as W
-        inputs = make_2d_inputs(side, fams or W.FAMILIES_8192, seed=10 + 17 * rank)
+        inputs = make_2d_inputs(side, fams or W.FAMILIES_8192, seed=replicas.replica_seed(10, rank))
         stages = STAGES_2D
         metric, unit = f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "Gpx/s"
 
@@ -283,16 +285,7 @@ def bench_ours(args, rank, world, local_rank):
     for s_, ms_ in enumerate(step_ms):
         per_image.setdefault(inputs[s_ % len(inputs)][0], []).append(ms_)
     per_image = {k: round(float(np.mean(v)), 4) for k, v in per_image.items()}
-    t_ms = float(sum(step_ms))
-    if world > 1:
-        tt = torch.tensor([t_ms], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_ms = float(tt.item())
-        pp = torch.tensor([float(px_done)], device=dev)
-        torch.distributed.all_reduce(pp, op=torch.distributed.ReduceOp.SUM)
-        px_total = float(pp.item())
-    else:
-        px_total = float(px_done)
+    t_ms, px_total = replicas.combine(float(sum(step_ms)), float(px_done), device=dev)
     value = px_total / (t_ms / 1e3) / 1e9
 
     # End to end through the host-buffer C-ABI call, pinned host memory.
@@ -429,11 +422,8 @@ def bench_batch(args, rank, world, local_rank):
         p1.record(stream)
         torch.cuda.synchronize()
         plain_ms = p0.elapsed_time(p1)
-    if world > 1:
-        tt = torch.tensor([t_ms], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_ms = float(tt.item())
-    value = world * npx * args.steps / (t_ms / 1e3) / 1e9
+    t_ms, px_all = replicas.combine(t_ms, float(npx * args.steps), device=dev)
+    value = px_all / (t_ms / 1e3) / 1e9
     plain = npx / (plain_ms / 1e3) / 1e9
     # end to end: pinned host images -> device -> batch graph -> labels back to pinned host
     h_in = [x.cpu().pin_memory() for x in d_in]
@@ -583,9 +573,7 @@ def main():
     ap.add_argument("--pool", type=int, default=40, help="serve: pre-generated requests")
     args = ap.parse_args()
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local_rank = replicas.rank_info()
     if args.impl == "reference":
         res = bench_reference(args, rank, world)
         if res is not None:
