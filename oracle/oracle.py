@@ -262,9 +262,21 @@ def ref_cpu_label2d(img: np.ndarray, alg: str = "bleq", thr: int = 0, threads: i
     return out, float(us.value)
 
 
-def ref_cpu_bleq(img: np.ndarray, thr: int = 0, threads: int = 0) -> Tuple[np.ndarray, float]:
-    """The reference's CPU block-equivalence labeler (the `bleq` CPU slot, main.cpp:122-126)."""
-    return ref_cpu_label2d(img, "bleq", thr, threads, 1)
+def ref_cpu_bleq(img: np.ndarray, thr: int = 0, threads: int = 0, pad: bool = True) -> Tuple[np.ndarray, float]:
+    """The reference's CPU block-equivalence labeler (the `bleq` CPU slot, main.cpp:122-126).
+
+    With `pad` (the default) the image gets one background row and column at its end before the
+    call and the labels are cropped back: that keeps the labeler's right- and bottom-border
+    probes inside background, and its labels are then exact (the padding is outside the
+    reference's stopwatch, which covers DoLabel only)."""
+    img = _u8(img)
+    if not pad:
+        return ref_cpu_label2d(img, "bleq", thr, threads, 1)
+    h, w = img.shape
+    padded = np.zeros((h + 1, w + 1), np.uint8)
+    padded[:h, :w] = img
+    lab, us = ref_cpu_label2d(padded, "bleq", thr, threads, 1)
+    return np.ascontiguousarray(lab[:h, :w]), us
 
 
 def ref_grana(img: np.ndarray, thr: int = 0) -> Tuple[np.ndarray, int]:

@@ -93,14 +93,14 @@ needs_ref_kernels = pytest.mark.skipif(O.ref_lib() is None, reason="oracle/_ref/
 
 @needs_ref_cpu
 @pytest.mark.parametrize("seed", range(4))
-def test_reference_cpu_bleq_matches_oracle_inside_a_background_frame(seed):
+def test_reference_cpu_bleq_matches_oracle_with_one_background_row_and_column(seed):
     """The reference's OpenMP block labeler (TLabelEquivalenceX2, the CPU baseline) gives the
-    oracle's partition once its border probes cannot wrap: a 2-pixel background frame."""
+    oracle's partition once its border probes cannot wrap: one background row and column
+    appended (how the baseline is run), any size, odd or even."""
     rng = np.random.default_rng(seed)
-    for _ in range(20):
-        h, w = rng.integers(1, 60, 2) * 2
-        img = np.zeros((h + 4, w + 4), np.uint8)
-        img[2:-2, 2:-2] = (rng.random((h, w)) < rng.uniform(0.2, 0.8)) * 255
+    for _ in range(25):
+        h, w = rng.integers(1, 90, 2)
+        img = ((rng.random((h, w)) < rng.uniform(0.2, 0.8)) * 255).astype(np.uint8)
         raw, us = O.ref_cpu_bleq(img)
         assert np.array_equal(O.canon(raw)[0], O.ccl2d(img)[0]) and us >= 0
 
@@ -112,7 +112,7 @@ def test_reference_cpu_bleq_right_border_wrap_is_the_references():
     in this 4 x 2 image the two components come out as one.  The GPU path follows the reference's
     GPU kernels, which pad the image and do not wrap."""
     img = np.array([[1, 0], [0, 0], [1, 1], [1, 0]], np.uint8) * 255
-    raw, _ = O.ref_cpu_bleq(img)
+    raw, _ = O.ref_cpu_bleq(img, pad=False)
     assert O.canon(raw)[1] == 1 and O.ccl2d(img)[1] == 2
 
 
