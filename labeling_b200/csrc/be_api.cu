@@ -171,7 +171,7 @@ cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persist
     Work wk = w;
     if (!persistent) wk.queue = nullptr;
     mark(0);
-    k_tile_local_3d<<<grid(w.n_tiles, 2), kT3Threads, 0, s>>>(L, wk);
+    k_tile_local_3d<<<grid(w.n_tiles, 5), kT3LocalThreads, 0, s>>>(L, wk);
     mark(1);
     k_merge_3d<<<grid(w.n_tiles, 8), kT3MergeThreads, 0, s>>>(L, wk);
     mark(2);

@@ -39,51 +39,17 @@ constexpr int NBLK = T3_NBLK;
 constexpr int NPERIM = T3_NPERIM;
 constexpr int MAXB = T3_MAXB;
 constexpr int NT = kT3Threads;
-constexpr int ZG = TB2 / 8;                 // 8-block groups along d2
-constexpr int ITEMS = TB0 * TB1 * ZG;       // items of 8 blocks
 constexpr int RBW = TZ / 32;                // root-bitmap words per voxel row
 constexpr uint32_t ROOT_FLAG = 1u << 23;
-constexpr int MQ3CAP = NBLK;                // merge-queue capacity (pairs per round)
 
 static_assert(NBLK <= (1 << 13), "tile-local block index must fit the entry payload");
 static_assert(TX * TY * TZ <= (1 << 23), "tile-local key must fit the entry payload");
-static_assert(ITEMS % NT == 0, "items must divide evenly");
 static_assert(NPERIM < 65536 && MAXB < 4096, "border encodings");
-
-// Voxel-offset selector of a block side along one axis: offset 0 (d = -1), 1 (d = +1) or both.
-__device__ __forceinline__ uint32_t sel_axis(int axis, int d)
-{
-    // bit v = 4i + 2j + k; axis 0 -> i, 1 -> j, 2 -> k
-    constexpr uint32_t lo[3] = {0x0Fu, 0x33u, 0x55u};
-    constexpr uint32_t hi[3] = {0xF0u, 0xCCu, 0xAAu};
-    return d < 0 ? lo[axis] : d > 0 ? hi[axis] : 0xFFu;
-}
-
-__device__ __forceinline__ uint32_t side_sel(int dx, int dy, int dz)
-{
-    return sel_axis(0, dx) & sel_axis(1, dy) & sel_axis(2, dz);
-}
-
-__device__ __forceinline__ bool bconn(uint32_t ma, uint32_t mb, int dx, int dy, int dz)
-{
-    return (ma & side_sel(dx, dy, dz)) && (mb & side_sel(-dx, -dy, -dz));
-}
 
 __device__ __forceinline__ int blk(int b0, int b1, int b2) { return (b0 * TB1 + b1) * TB2 + b2; }
 
-// Byte-packed mask words: byte k = mask of block k.  nzb gives bit 8k = (byte k != 0);
-// rep8 repeats a byte selector in all eight bytes.
-__device__ __forceinline__ uint64_t nzb(uint64_t x)
-{
-    x |= x >> 4;
-    x |= x >> 2;
-    x |= x >> 1;
-    return x & 0x0101010101010101ull;
-}
-__device__ __forceinline__ uint64_t rep8(uint32_t sel) { return uint64_t(sel) * 0x0101010101010101ull; }
-
-// Out-of-line merge keeps the kernel's code small.
-__device__ __noinline__ void merge_blocks3(uint32_t *P, uint32_t a, uint32_t b) { smerge(P, a, b); }
+// Highest set bit of x (x != 0).
+__device__ __forceinline__ uint32_t hibit3(uint32_t x) { return 31u - __clz(x); }
 
 // Tile-local key of the first voxel of a block.
 __device__ __forceinline__ uint32_t local_key(int b, uint32_t m)
@@ -92,21 +58,6 @@ __device__ __forceinline__ uint32_t local_key(int b, uint32_t m)
     const int b2 = b % TB2, b1 = (b / TB2) % TB1, b0 = b / (TB1 * TB2);
     const int X = 2 * b0 + (v >> 2), Y = 2 * b1 + ((v >> 1) & 1), Z = 2 * b2 + (v & 1);
     return uint32_t((X * TY + Y) * TZ + Z);
-}
-
-__device__ __forceinline__ uint32_t nib2byte(uint32_t x)
-{
-    x &= 0xFFFFu;
-    x = (x | (x << 8)) & 0x00FF00FFu;
-    x = (x | (x << 4)) & 0x0F0F0F0Fu;
-    return x;
-}
-
-// 16 foreground bits along d2 (8 blocks x 2 voxels) -> per block 2-bit field in its byte.
-__device__ __forceinline__ uint2 pairs_to_bytes(uint32_t bits16)
-{
-    const uint32_t n = pairs_to_nibbles(bits16);
-    return make_uint2(nib2byte(n), nib2byte(n >> 16));
 }
 
 // Border faces: 0 = -d0, 1 = +d0, 2 = -d1, 3 = +d1, 4 = -d2, 5 = +d2.
@@ -178,228 +129,333 @@ __device__ __forceinline__ bool perim_pos3(int p, const TileGeo &g, int &f, int 
 }  // namespace
 
 // ---------------------------------------------------------------------------------------------
-// Tile-local labeling.
+// Tile-local labeling.  One thread per block row along d2: the tile is TB2 = 32 blocks deep, so a
+// row is one 32-bit word per voxel class (v = 4i + 2j + k, the voxel's offsets in its block).
+// Faces, runs along d2, run starts and the links to the four preceding rows are bit operations;
+// only runs enter the union-find, ordered by the raster position of their first voxel.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT, 4) k_tile_local_3d(ImgList3D L, Work w)
+namespace {
+
+constexpr int NT1 = kT3LocalThreads;   // threads of the tile-local kernel: one per block row
+constexpr int MQ1 = 2048;          // merge-queue capacity per round (more are merged in place)
+static_assert(TB2 == 32, "a block row along d2 is one 32-bit word");
+static_assert(NBLK <= 4096, "run starts must fit 12 bits");
+
+// Word of the blocks whose side toward (dx, dy, dz) holds a foreground voxel: the OR of the
+// classes with offset 0 along an axis where d < 0, offset 1 where d > 0.
+template <int DX, int DY, int DZ>
+__device__ __forceinline__ uint32_t face_word(const uint32_t (&c)[8])
 {
-    __shared__ uint32_t P[NBLK];
-    __shared__ uint32_t KQ[NBLK];   // merge queue in Phase B, then first-voxel keys (KM)
-    uint32_t *const MQ3 = KQ, *const KM = KQ;
-    __shared__ __align__(16) uint8_t M[NBLK];
+    uint32_t r = 0;
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+        const int i = v >> 2, j = (v >> 1) & 1, k = v & 1;
+        if ((DX < 0 && i) || (DX > 0 && !i) || (DY < 0 && j) || (DY > 0 && !j) || (DZ < 0 && k) || (DZ > 0 && !k))
+            continue;
+        r |= c[v];
+    }
+    return r;
+}
+
+// Slot of a block with first voxel offsets (i, j): the raster order of first voxels is the order
+// of (b0, i, b1, j, b2) (b2 decides last: blocks of one row and class differ only there).
+__device__ __forceinline__ uint32_t slot3(int b0, int i, int b1, int j, int b2)
+{
+    return uint32_t((((b0 * 2 + i) * TB1 + b1) * 2 + j) * TB2 + b2);
+}
+
+__device__ __forceinline__ uint32_t slot_block(uint32_t slot)
+{
+    const uint32_t b2 = slot % TB2, b1 = (slot / (2 * TB2)) % TB1, b0 = slot / (4 * TB2 * TB1);
+    return (b0 * TB1 + b1) * TB2 + b2;
+}
+
+// Union-find over run starts, the slot carried in the entry: (slot << 12) | parent.
+__device__ __forceinline__ uint32_t efind3(uint32_t *P, uint32_t x)
+{
+    uint32_t v = P[x];
+    while ((v & 0xFFFu) != x) {
+        const uint32_t y = v & 0xFFFu;
+        const uint32_t vg = P[y];
+        if ((vg & 0xFFFu) != y) P[x] = vg;
+        x = y;
+        v = vg;
+    }
+    return x;
+}
+
+__device__ __forceinline__ uint32_t efind3_ro(const uint32_t *P, uint32_t x)
+{
+    uint32_t v = P[x];
+    while ((v & 0xFFFu) != x) {
+        x = v & 0xFFFu;
+        v = P[x];
+    }
+    return x;
+}
+
+__device__ __forceinline__ void eunion3(uint32_t *P, uint32_t a, uint32_t b)
+{
+    for (;;) {
+        a = efind3(P, a);
+        b = efind3(P, b);
+        if (a == b) return;
+        const uint32_t ea = P[a], eb = P[b];
+        if (ea < eb) {
+            const uint32_t old = atomicMin(&P[b], ea);
+            if ((old & 0xFFFu) == b) return;
+            b = old & 0xFFFu;
+        } else {
+            const uint32_t old = atomicMin(&P[a], eb);
+            if ((old & 0xFFFu) == a) return;
+            a = old & 0xFFFu;
+        }
+    }
+}
+
+// Bits 0..3 of x -> bit 0 of bytes 0..3.
+__device__ __forceinline__ uint32_t spread4b(uint32_t x) { return ((x & 0xFu) * 0x00204081u) & 0x01010101u; }
+
+// Byte-wise x > thr (bit 7 of each byte); K = 0x7F - (thr & 0x7F) per byte, hi = thr >= 128.
+__device__ __forceinline__ uint32_t gt_bytes3(uint32_t x, uint32_t K, bool hi)
+{
+    const uint32_t s = (x & 0x7F7F7F7Fu) + K;
+    return (hi ? (x & s) : (x | s)) & 0x80808080u;
+}
+__device__ __forceinline__ uint32_t gather4b(uint32_t g) { return (g * 0x00204081u) >> 28; }
+
+// 16 voxels along d2 -> foreground bits of the even (k = 0) and odd (k = 1) voxels: 8 blocks.
+__device__ __forceinline__ void split16b(uint4 v, uint32_t K, bool hi, uint32_t &ev, uint32_t &od)
+{
+    ev = gather4b(gt_bytes3(__byte_perm(v.x, v.y, 0x6420), K, hi)) |
+         (gather4b(gt_bytes3(__byte_perm(v.z, v.w, 0x6420), K, hi)) << 4);
+    od = gather4b(gt_bytes3(__byte_perm(v.x, v.y, 0x7531), K, hi)) |
+         (gather4b(gt_bytes3(__byte_perm(v.z, v.w, 0x7531), K, hi)) << 4);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
+{
+    __shared__ uint32_t P[NBLK];               // run starts: (slot << 12) | parent
+    __shared__ __align__(16) uint8_t M[NBLK];  // block masks
+    __shared__ uint32_t CW[8][NT1];            // class words of every row
+    __shared__ uint32_t WHZ[NT1], WS[NT1];     // joins along d2, run starts
     __shared__ uint32_t RB[TX * TY * RBW];
     __shared__ uint32_t BF[NBLK / 32];
     __shared__ uint32_t BP[NBLK / 32];
-    __shared__ uint32_t tmp[NT / 32 + 1];
-    __shared__ uint32_t mqn3[4 * (ITEMS / NT)];      // queue length of each round
+    __shared__ uint32_t MQ[MQ1];               // merge queue: (start_a << 16) | start_b
+    __shared__ uint32_t mqn[4];
+    __shared__ uint32_t tmp[NT1 / 32 + 1];
     __shared__ uint32_t qslot;
 
     const int tid = threadIdx.x;
+    const int b0 = tid / TB1, b1 = tid % TB1;
+    const uint32_t rowb = uint32_t(tid) * TB2;   // block index of the row's first block
     uint32_t *lab = reinterpret_cast<uint32_t *>(w.lab);
     ItemLoop loop{w.queue ? w.queue + 0 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
         const Img3D im = L.get(t);
         const TileGeo g = tile_geo(im, t);
-        const uint32_t thr4 = uint32_t(im.thr) * 0x01010101u;
+        const uint32_t K = (0x7Fu - (uint32_t(im.thr) & 0x7Fu)) * 0x01010101u;
+        const bool hi = im.thr >= 128;
         const int64_t rs0 = int64_t(im.d1) * im.d2;   // stride of d0 in voxels
 
-        for (int i = tid; i < TX * TY * RBW; i += NT) RB[i] = 0;
-        if (tid < NBLK / 32) BF[tid] = 0;
-        if (tid < 4 * (ITEMS / NT)) mqn3[tid] = 0;
+        for (int i = tid; i < TX * TY * RBW; i += NT1) RB[i] = 0;
+        BF[tid] = 0;
+        if (tid < 4) mqn[tid] = 0;
 
-        // Phase A: masks and runs along d2.
-        uint64_t masks[ITEMS / NT];
+        // Phase A: class words, runs along d2, run slots.
+        uint32_t c[8];
 #pragma unroll
-        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
-            const int it = tid + it_i * NT;
-            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
-            uint2 acc = make_uint2(0, 0);
-            if (b0 < g.n0 && b1 < g.n1 && 16 * zg < g.nz) {
-                const int zz = g.z0 + 16 * zg;
-                const int n = min(16, g.nz - 16 * zg);
+        for (int v = 0; v < 8; ++v) c[v] = 0;
+        if (b0 < g.n0 && b1 < g.n1) {
 #pragma unroll
-                for (int ij = 0; ij < 4; ++ij) {
-                    const int i = ij >> 1, j = ij & 1;
-                    const int X = g.x0 + 2 * b0 + i, Y = g.y0 + 2 * b1 + j;
-                    if (X >= im.d0 || Y >= im.d1) continue;
-                    const uint8_t *row = im.in + X * rs0 + int64_t(Y) * im.d2 + zz;
-                    uint32_t bits = 0;
-                    if (n == 16 && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
-                        bits = fg16(__ldg(reinterpret_cast<const uint4 *>(row)), thr4);
-                    } else {
-                        for (int z = 0; z < n; ++z) bits |= uint32_t(row[z] > im.thr) << z;
+            for (int ij = 0; ij < 4; ++ij) {
+                const int i = ij >> 1, j = ij & 1;
+                const int X = 2 * b0 + i, Y = 2 * b1 + j;
+                if (X >= g.nx || Y >= g.ny) continue;
+                const uint8_t *row = im.in + (g.x0 + X) * rs0 + int64_t(g.y0 + Y) * im.d2 + g.z0;
+                uint32_t ev = 0, od = 0;
+                if (g.nz == TZ && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+                    const uint4 *pv = reinterpret_cast<const uint4 *>(row);
+                    uint4 q[4];
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) q[h] = __ldg(pv + h);
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) {
+                        uint32_t e8, o8;
+                        split16b(q[h], K, hi, e8, o8);
+                        ev |= e8 << (8 * h);
+                        od |= o8 << (8 * h);
                     }
-                    const uint2 pb = pairs_to_bytes(bits);
-                    const int sh = 4 * i + 2 * j;
-                    acc.x |= pb.x << sh;
-                    acc.y |= pb.y << sh;
-                }
-            }
-            masks[it_i] = (uint64_t(acc.y) << 32) | acc.x;
-            const int bb = blk(b0, b1, 8 * zg);
-            *reinterpret_cast<uint2 *>(&M[bb]) = acc;
-            uint32_t run = 0;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t m = uint32_t(masks[it_i] >> (8 * k)) & 0xFFu;
-                if (!m) continue;
-                const uint32_t mp = k ? uint32_t(masks[it_i] >> (8 * (k - 1))) & 0xFFu : 0u;
-                if (!(k && bconn(m, mp, 0, 0, -1))) run = bb + k;
-                P[bb + k] = run;
-            }
-        }
-        __syncthreads();
-
-        // Phase B: merges with the 13 preceding neighbours inside the tile, decided for the 8
-        // blocks of a group at once on byte-packed masks (bit 8k = block k): the 12 neighbours
-        // in the four preceding rows (d0-1, d1-1 / d0-1, d1 / d0-1, d1+1 / d0, d1-1) and, at the
-        // group's first block, the block before it along d2.  One round per (item, row): every
-        // lane queues its links in shared memory, then all lanes merge the queue, so lanes with
-        // many links do not hold up their warp.  A round queues at most NT * (3 * 8 + 1) pairs;
-        // the queue holds NBLK (it shares its memory with the keys of Phase C), and pairs beyond
-        // it are merged in place.
-#pragma unroll
-        for (int it_i = 0; it_i < ITEMS / NT; ++it_i)
-#pragma unroll 1
-        for (int row = 0; row < 4; ++row) {
-            const int round = 4 * it_i + row;
-            const int it = tid + it_i * NT;
-            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
-            const uint64_t ms = masks[it_i];
-            const int bb = blk(b0, b1, 8 * zg);
-            const int dx = row < 3 ? -1 : 0, dy = row < 3 ? row - 1 : -1;
-            const int n0 = b0 + dx, n1 = b1 + dy;
-            const int nb0 = (n0 >= 0 && n1 >= 0 && n1 < TB1) ? blk(n0, n1, 8 * zg) : -1;
-            uint64_t c[3] = {0, 0, 0};
-            bool link_z = false;
-            if (ms) {
-                const uint64_t ML = zg > 0 ? M[bb - 1] : 0u;
-                // hz: block k is joined along d2 to block k-1 (same run)
-                const uint64_t hz = nzb(ms & rep8(side_sel(0, 0, -1))) &
-                                    nzb(((ms << 8) | ML) & rep8(side_sel(0, 0, 1)));
-                link_z = row == 0 && (hz & 1u);
-                if (nb0 >= 0) {
-                    const uint2 nv = *reinterpret_cast<const uint2 *>(&M[nb0]);
-                    const uint64_t N = (uint64_t(nv.y) << 32) | nv.x;
-                    const uint64_t NL = zg > 0 ? M[nb0 - 1] : 0u;
-                    const uint64_t NR = 8 * zg + 8 < TB2 ? M[nb0 + 8] : 0u;
-                    if (N | NL | NR) {
-#pragma unroll
-                        for (int dz = -1; dz <= 1; ++dz) {
-                            const uint64_t Ns = dz < 0 ? (N << 8) | NL : dz > 0 ? (N >> 8) | (NR << 56) : N;
-                            c[dz + 1] = nzb(ms & rep8(side_sel(dx, dy, dz))) &
-                                        nzb(Ns & rep8(side_sel(-dx, -dy, -dz)));
-                        }
-                        // Skip rules (as in the 2D kernel: every chain of reasons runs toward
-                        // smaller d2 along the run and ends at a link that is made).
-                        // (1) The previous block of the run touches the same block of row N.
-                        const uint64_t raw1 = c[1];
-                        c[0] &= ~(hz & (raw1 << 8));
-                        c[1] &= ~(hz & (c[2] << 8));
-                        // (2) Blocks of row N joined along d2 to the block this one touches
-                        //     with dz = 0.
-                        const uint64_t hzN = nzb(N & rep8(side_sel(0, 0, -1))) &
-                                             nzb(((N << 8) | NL) & rep8(side_sel(0, 0, 1)));
-                        const uint64_t hzN1 =
-                            (hzN >> 8) |
-                            (uint64_t((NR & side_sel(0, 0, -1)) && ((N >> 56) & side_sel(0, 0, 1))) << 56);
-                        c[0] &= ~(raw1 & hzN);
-                        c[2] &= ~(raw1 & hzN1);
+                } else {
+                    for (int z = 0; z < g.nz; ++z) {
+                        const uint32_t bit = uint32_t(row[z] > im.thr) << (z >> 1);
+                        if (z & 1) od |= bit;
+                        else ev |= bit;
                     }
                 }
+                c[4 * i + 2 * j] = ev;
+                c[4 * i + 2 * j + 1] = od;
             }
-            const uint32_t n = __popcll(c[0]) + __popcll(c[1]) + __popcll(c[2]) + (link_z ? 1u : 0u);
-            uint32_t pos = warp_reserve(&mqn3[round], n);
-            auto push = [&](uint32_t x, uint32_t y) {
-                if (pos < uint32_t(MQ3CAP)) MQ3[pos] = (x << 16) | y;
-                else smerge(P, x, y);   // queue full: merge in place
-                ++pos;
-            };
-            if (link_z) push(uint32_t(bb), uint32_t(bb - 1));
-            uint64_t todo = c[0] | c[1] | c[2];
-            while (todo) {
-                const int k = (__ffsll(todo) - 1) >> 3;
-                const uint64_t bit = uint64_t(1) << (8 * k);
-                todo &= ~bit;
-                if (c[0] & bit) push(uint32_t(bb + k), uint32_t(nb0 + k - 1));
-                if (c[1] & bit) push(uint32_t(bb + k), uint32_t(nb0 + k));
-                if (c[2] & bit) push(uint32_t(bb + k), uint32_t(nb0 + k + 1));
+        }
+        const uint32_t Fw = c[0] | c[1] | c[2] | c[3] | c[4] | c[5] | c[6] | c[7];
+        const uint32_t hz = face_word<0, 0, 1>(c) & (face_word<0, 0, -1>(c) >> 1);   // k joined to k + 1
+        const uint32_t hl = hz << 1;                                               // k joined to k - 1
+        const uint32_t S = Fw & ~hl;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) CW[v][tid] = c[v];
+        WHZ[tid] = hz;
+        WS[tid] = S;
+        {
+            uint32_t mw[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                uint32_t m = 0;
+#pragma unroll
+                for (int v = 0; v < 8; ++v) m |= spread4b(c[v] >> (4 * q)) << v;
+                mw[q] = m;
+            }
+            uint4 *md = reinterpret_cast<uint4 *>(&M[rowb]);
+            md[0] = make_uint4(mw[0], mw[1], mw[2], mw[3]);
+            md[1] = make_uint4(mw[4], mw[5], mw[6], mw[7]);
+        }
+        {
+            const uint32_t H00 = c[0] | c[1], H01 = c[2] | c[3], H10 = c[4] | c[5], H11 = c[6] | c[7];
+            uint32_t ss = S;
+            while (ss) {
+                const uint32_t s0 = __ffs(ss) - 1;
+                ss &= ss - 1;
+                const uint32_t from = ~0u << s0;
+                const uint32_t brk = ~hz & from;
+                const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
+                const uint32_t span = from & ((2u << e) - 1u);
+                int i, j;
+                uint32_t m;
+                if (H00 & span) { i = 0; j = 0; m = H00 & span; }
+                else if (H01 & span) { i = 0; j = 1; m = H01 & span; }
+                else if (H10 & span) { i = 1; j = 0; m = H10 & span; }
+                else { i = 1; j = 1; m = H11 & span; }
+                const uint32_t x = rowb + s0;
+                P[x] = (slot3(b0, i, b1, j, __ffs(m) - 1) << 12) | x;
+            }
+        }
+        __syncthreads();
+
+        // Phase B: links to the four preceding rows (d0-1 with d1-1 / d1 / d1+1, and d0 with
+        // d1-1), each with offsets dz = -1 / 0 / +1 along d2.  As in 2D, a link is dropped when
+        // an earlier one (further along d2, or dz = 0 before dz = +-1 at the same block) joins the
+        // same two runs.  One round per neighbour row: queue, then merge with every lane.
+#pragma unroll
+        for (int nr = 0; nr < 4; ++nr) {
+            const int dx = nr < 3 ? -1 : 0, dy = nr < 3 ? nr - 1 : -1;
+            const int r0 = b0 + dx, r1 = b1 + dy;
+            uint32_t N = 0, NW = 0, NE = 0, uS = 0;
+            int ur = 0;
+            if (Fw && r0 >= 0 && r1 >= 0 && r1 < TB1) {
+                ur = r0 * TB1 + r1;
+                uint32_t u[8];
+#pragma unroll
+                for (int v = 0; v < 8; ++v) u[v] = CW[v][ur];
+                uint32_t A0, Am, Ap, B0, Bm, Bp;   // own sides toward dz = 0/-1/+1, neighbour's opposite sides
+                if (nr == 0) {
+                    A0 = face_word<-1, -1, 0>(c); Am = face_word<-1, -1, -1>(c); Ap = face_word<-1, -1, 1>(c);
+                    B0 = face_word<1, 1, 0>(u); Bm = face_word<1, 1, 1>(u); Bp = face_word<1, 1, -1>(u);
+                } else if (nr == 1) {
+                    A0 = face_word<-1, 0, 0>(c); Am = face_word<-1, 0, -1>(c); Ap = face_word<-1, 0, 1>(c);
+                    B0 = face_word<1, 0, 0>(u); Bm = face_word<1, 0, 1>(u); Bp = face_word<1, 0, -1>(u);
+                } else if (nr == 2) {
+                    A0 = face_word<-1, 1, 0>(c); Am = face_word<-1, 1, -1>(c); Ap = face_word<-1, 1, 1>(c);
+                    B0 = face_word<1, -1, 0>(u); Bm = face_word<1, -1, 1>(u); Bp = face_word<1, -1, -1>(u);
+                } else {
+                    A0 = face_word<0, -1, 0>(c); Am = face_word<0, -1, -1>(c); Ap = face_word<0, -1, 1>(c);
+                    B0 = face_word<0, 1, 0>(u); Bm = face_word<0, 1, 1>(u); Bp = face_word<0, 1, -1>(u);
+                }
+                const uint32_t uhz = WHZ[ur], uhl = uhz << 1;
+                uS = WS[ur];
+                const uint32_t n0 = A0 & B0, nw = Am & (Bm << 1), ne = Ap & (Bp >> 1);
+                const uint32_t Nsh = n0 << 1, NEsh = ne << 1;
+                N = n0 & ~(hl & ((Nsh & uhl) | NEsh));
+                NW = nw & ~((n0 & uhl) | (hl & Nsh));
+                NE = ne & ~((n0 & uhz) | (hl & NEsh & uhz));
+            }
+            const uint32_t n = __popc(N) + __popc(NW) + __popc(NE);
+            uint32_t pos = warp_reserve(&mqn[nr], n);
+            {
+                const uint32_t ubase = uint32_t(ur) * TB2;
+                auto push = [&](uint32_t a, uint32_t b) {
+                    if (pos < uint32_t(MQ1)) MQ[pos] = (a << 16) | b;
+                    else eunion3(P, a, b);   // queue full: merge in place
+                    ++pos;
+                };
+                uint32_t todo = N | NW | NE;
+                while (todo) {
+                    const uint32_t k = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    const uint32_t bit = 1u << k;
+                    const uint32_t a = rowb + hibit3(S & ((2u << k) - 1u));
+                    if (N & bit) push(a, ubase + hibit3(uS & ((2u << k) - 1u)));
+                    if (NW & bit) push(a, ubase + hibit3(uS & ((1u << k) - 1u)));
+                    if (NE & bit) push(a, ubase + hibit3(uS & ((4u << k) - 1u)));
+                }
             }
             __syncthreads();
-            const uint32_t nq = min(mqn3[round], uint32_t(MQ3CAP));
-            for (uint32_t q = tid; q < nq; q += NT) smerge(P, MQ3[q] >> 16, MQ3[q] & 0xFFFFu);
+            const uint32_t nq = min(mqn[nr], uint32_t(MQ1));
+            for (uint32_t q = tid; q < nq; q += NT1) eunion3(P, MQ[q] >> 16, MQ[q] & 0xFFFFu);
             __syncthreads();
         }
 
-        // Phase C: roots (read-only finds: all merges are done) and per-component first-voxel
-        // key.  Each root first stores its own block's key; a block of the component then needs
-        // the atomic only when its key is smaller, which keeps the atomics off the (common) case
-        // of a large component whose blocks all follow its root block.
-        uint16_t roots[ITEMS / NT][8];
-#pragma unroll
-        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
-            const int it = tid + it_i * NT;
-            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
-            const uint64_t ms = masks[it_i];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
-                if (!m) continue;
-                const int b = blk(b0, b1, 8 * zg + k);
-                const uint32_t root = sflatten(P, b);
-                roots[it_i][k] = uint16_t(root);
-                if (root == uint32_t(b)) KM[b] = local_key(b, m);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
-            const int it = tid + it_i * NT;
-            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
-            const uint64_t ms = masks[it_i];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
-                if (!m) continue;
-                const int b = blk(b0, b1, 8 * zg + k);
-                const uint32_t root = roots[it_i][k];
-                if (root == uint32_t(b)) continue;
-                const uint32_t key = local_key(b, m);
-                if (key < KM[root]) atomicMin(&KM[root], key);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int it_i = 0; it_i < ITEMS / NT; ++it_i) {
-            const int it = tid + it_i * NT;
-            const int zg = it % ZG, b1 = (it / ZG) % TB1, b0 = it / (ZG * TB1);
-            const uint64_t ms = masks[it_i];
-            const int bb = blk(b0, b1, 8 * zg);
-            uint32_t e[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t m = uint32_t(ms >> (8 * k)) & 0xFFu;
-                e[k] = 0;
-                if (!m) continue;
-                const int b = bb + k;
-                const uint32_t root = roots[it_i][k];
-                if (root == uint32_t(b)) {
-                    const uint32_t key = KM[b];
-                    e[k] = (m << 24) | ROOT_FLAG | key;
+        // Phase C: every run start points straight at its root; roots mark their first voxel.
+        {
+            uint32_t ss = S;
+            while (ss) {
+                const uint32_t s0 = __ffs(ss) - 1;
+                ss &= ss - 1;
+                const uint32_t x = rowb + s0;
+                const uint32_t root = efind3_ro(P, x);
+                const uint32_t ev = P[root];
+                for (uint32_t y = x; y != root;) {
+                    const uint32_t ny = P[y] & 0xFFFu;
+                    P[y] = ev;
+                    y = ny;
+                }
+                if (root == x) {
+                    const uint32_t rb = slot_block(ev >> 12);
+                    const uint32_t key = local_key(int(rb), M[rb]);
                     const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
                     if (GUARD(w, key < uint32_t(TX * TY * TZ), 101, key))
                         atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
-                } else {
-                    e[k] = (m << 24) | root;
                 }
             }
-            uint4 *dst = reinterpret_cast<uint4 *>(lab + t * NBLK + bb);
-            dst[0] = make_uint4(e[0], e[1], e[2], e[3]);
-            dst[1] = make_uint4(e[4], e[5], e[6], e[7]);
         }
         __syncthreads();
+        // Block entries: the root block of a component carries ROOT_FLAG | its first-voxel key,
+        // every other block its root block.
+        {
+            uint32_t cur = 0;
+#pragma unroll
+            for (int h = 0; h < 8; ++h) {
+                const uint32_t mm = *reinterpret_cast<const uint32_t *>(&M[rowb + 4 * h]);
+                uint32_t e[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int k = 4 * h + q;
+                    if ((S >> k) & 1u) cur = slot_block(P[rowb + k] >> 12);
+                    const uint32_t m = (mm >> (8 * q)) & 0xFFu;
+                    uint32_t v = 0;
+                    if (m) {
+                        v = (m << 24) | cur;
+                        if (cur == rowb + uint32_t(k)) v = (m << 24) | ROOT_FLAG | local_key(int(cur), m);
+                    }
+                    e[q] = v;
+                }
+                reinterpret_cast<uint4 *>(lab + t * NBLK + rowb)[h] = make_uint4(e[0], e[1], e[2], e[3]);
+            }
+        }
 
         // Phase D: segment counts and border nodes.
-        for (int r = tid; r < TX * TY; r += NT) {
+        for (int r = tid; r < TX * TY; r += NT1) {
             const int X = r / TY, Y = r % TY;
             if (X >= g.nx || Y >= g.ny) continue;
             uint32_t cnt = 0;
@@ -408,27 +464,32 @@ __global__ void __launch_bounds__(NT, 4) k_tile_local_3d(ImgList3D L, Work w)
             const int64_t si = im.seg_base + (int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.t2 + g.tx2;
             if (GUARD(w, si >= 0 && si < w.n_segs, 104, si)) w.segcnt[si] = uint8_t(cnt);
         }
-        for (int p = tid; p < NPERIM; p += NT) {
-            int f, b0, b1, b2;
-            if (!perim_pos3(p, g, f, b0, b1, b2)) continue;
-            const int b = blk(b0, b1, b2);
+        auto root_block = [&](int b) -> uint32_t {
+            const uint32_t row = uint32_t(b) >> 5, k = uint32_t(b) & 31u;
+            const uint32_t st = hibit3(WS[row] & ((2u << k) - 1u));
+            return slot_block(P[(row << 5) + st] >> 12);
+        };
+        for (int p = tid; p < NPERIM; p += NT1) {
+            int f, pb0, pb1, pb2;
+            if (!perim_pos3(p, g, f, pb0, pb1, pb2)) continue;
+            const int b = blk(pb0, pb1, pb2);
             if (!M[b]) continue;
-            const uint32_t rb = sfind_ro(P, b);
+            const uint32_t rb = root_block(b);
             atomicOr(&BF[rb >> 5], 1u << (rb & 31));
         }
         __syncthreads();
         uint32_t nb;
-        const uint32_t pre = block_exscan<NT>(tid < NBLK / 32 ? __popc(BF[tid]) : 0u, tmp, &nb);
-        if (tid < NBLK / 32) BP[tid] = pre;
+        const uint32_t pre = block_exscan<NT1>(__popc(BF[tid]), tmp, &nb);
+        BP[tid] = pre;
         __syncthreads();
-        if (tid < NBLK / 32) {
+        {
             uint32_t bits = BF[tid];
             uint32_t j = pre;
             while (bits) {
                 const int bit = __ffs(bits) - 1;
                 bits &= bits - 1;
                 const uint32_t rb = tid * 32 + bit;
-                const uint32_t key = KM[rb];
+                const uint32_t key = local_key(int(rb), M[rb]);
                 if (!GUARD(w, key < uint32_t(TX * TY * TZ) && j < uint32_t(MAXB), 102, (uint64_t(j) << 32) | key))
                     break;
                 const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
@@ -443,14 +504,14 @@ __global__ void __launch_bounds__(NT, 4) k_tile_local_3d(ImgList3D L, Work w)
                 ++j;
             }
         }
-        for (int p = tid; p < NPERIM; p += NT) {
-            int f, b0, b1, b2;
+        for (int p = tid; p < NPERIM; p += NT1) {
+            int f, pb0, pb1, pb2;
             uint16_t ent = 0;
-            if (perim_pos3(p, g, f, b0, b1, b2)) {
-                const int b = blk(b0, b1, b2);
+            if (perim_pos3(p, g, f, pb0, pb1, pb2)) {
+                const int b = blk(pb0, pb1, pb2);
                 const uint32_t m = M[b];
                 if (m) {
-                    const uint32_t rb = sfind_ro(P, b);
+                    const uint32_t rb = root_block(b);
                     const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
                     ent = uint16_t((j << 4) | face_bits(m, f));
                 }
