@@ -348,16 +348,28 @@ __global__ void __launch_bounds__(K1_NT, 5) k_tile_local_2d(ImgList2D L, Work w)
         __syncthreads();
 
         // Phase C: every run start points straight at its root; roots mark their first pixel.
+        // The starts are listed first (the merge queue is free again) and taken round robin, so
+        // the work is even over the lanes and a row's parents -- the row above, listed one
+        // round earlier -- are mostly already compressed when a row is walked.
+        if (tid == 0) mqn = 0;
+        __syncthreads();
         {
+            uint32_t pos = warp_reserve(&mqn, __popc(S));
             uint32_t ss = S;
             while (ss) {
                 const uint32_t s0 = __ffs(ss) - 1;
                 ss &= ss - 1;
-                const uint32_t x = rbase + 32 * q + s0;
+                MQ[pos++] = rbase + 32 * q + s0;
+            }
+        }
+        __syncthreads();
+        {
+            const uint32_t nruns = mqn;
+            for (uint32_t i = tid; i < nruns; i += K1_NT) {
+                const uint32_t x = MQ[i];
                 const uint32_t root = efind_ro(P, x);
                 const uint32_t ev = P[root];
-                // Point the whole path at the root (every writer stores the same final value), so
-                // the long chains of thin vertical lines are walked once.
+                // Point the whole path at the root (every writer stores the same final value).
                 for (uint32_t y = x; y != root;) {
                     const uint32_t ny = P[y] & 0xFFFu;
                     P[y] = ev;
