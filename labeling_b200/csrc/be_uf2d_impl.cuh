@@ -632,6 +632,16 @@ __device__ void post_tile_2d(const ImgList2D &L, Work &w, int64_t t)
     for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
         const int64_t node = t * MAXB + j;
         if (w.gp[node] == uint32_t(node)) continue;
+        // All unions are done: point the node's whole path at its root, so that the label pass
+        // (and the other tiles' walks here) find it in one step.
+        {
+            const uint32_t root = gfind_ro(w.gp, uint32_t(node));
+            for (uint32_t y = uint32_t(node); y != root;) {
+                const uint32_t ny = w.gp[y];
+                w.gp[y] = root;
+                y = ny;
+            }
+        }
         const uint32_t k = w.nkey[node];
         const uint32_t y = k / uint32_t(im.cols);
         const int ly = int(y) - y0, lx = int(k - y * uint32_t(im.cols)) - x0;

@@ -757,6 +757,16 @@ __device__ void post_tile_3d(const ImgList3D &L, Work &w, int64_t t)
     for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
         const int64_t node = t * MAXB + j;
         if (w.gp[node] == uint32_t(node)) continue;
+        // All unions are done: point the node's whole path at its root, so that the label pass
+        // (and the other tiles' walks here) find it in one step.
+        {
+            const uint32_t root = gfind_ro(w.gp, uint32_t(node));
+            for (uint32_t y = uint32_t(node); y != root;) {
+                const uint32_t ny = w.gp[y];
+                w.gp[y] = root;
+                y = ny;
+            }
+        }
         int X, Y, Z;
         local(w.nkey[node], X, Y, Z);
         if (GUARD(w, X >= 0 && X < TX && Y >= 0 && Y < TY && Z >= 0 && Z < TZ, 301, w.nkey[node]))
