@@ -57,18 +57,53 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region: NVML every
+    millisecond from a helper thread (the timed regions are tens of milliseconds long), with
+    nvidia-smi as the fallback.  Read-only: no GPU setting is changed."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.samples = []       # (sm_mhz, max_mhz, set of reasons)
+        self.nvml = None
+        self.stop = threading.Event()
+        self.t = None
+
+    def _nvml_sample(self):
+        n = self.nvml
+        sm = n.nvmlDeviceGetClockInfo(self.h, n.NVML_CLOCK_SM)
+        mx = n.nvmlDeviceGetMaxClockInfo(self.h, n.NVML_CLOCK_SM)
+        r = n.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        bits = [n.nvmlClocksEventReasonHwSlowdown, n.nvmlClocksEventReasonHwThermalSlowdown,
+                n.nvmlClocksEventReasonSwThermalSlowdown, n.nvmlClocksEventReasonSwPowerCap]
+        self.samples.append((float(sm), float(mx), {nm for nm, b in zip(self.NAMES, bits) if r & b}))
+
+    def _nvml_loop(self):
+        while not self.stop.is_set():
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
+            self.stop.wait(0.001)
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self._nvml_sample()
+            self.t = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
@@ -84,6 +119,15 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        if self.nvml is not None:
+            self.stop.set()
+            if self.t:
+                self.t.join(timeout=2)
+            try:
+                self._nvml_sample()
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -93,7 +137,10 @@ class ClockSampler:
 
     def summary(self):
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s_, m_, r_ in self.samples:
+            sm.append(s_)
+            mx = m_
+            reasons |= r_
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
@@ -103,13 +150,13 @@ class ClockSampler:
                 mx = float(f[2])
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
+            for n, v in zip(self.NAMES, f[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 # ------------------------------------------------------------------------------------------
@@ -491,8 +538,14 @@ def bench_serve(args, rank, world, local_rank):
         h_out = torch.empty(img.shape, dtype=torch.int32).pin_memory()
         pool.append((h_in.numpy(), h_out.numpy()))
     srv = be.Server(device=local_rank, lanes=2, max_batch=64)
-    for i in range(min(4, len(pool))):          # warm-up (pool allocations, first launches)
+    # Warm-up: single requests (first launches), then the whole pool at once, twice, so the
+    # device memory pool and the pinned descriptor staging reach their largest sizes before any
+    # rate is timed (growing them stalls the device once).
+    for i in range(min(4, len(pool))):
         srv.wait(srv.submit(*pool[i]))
+    for _ in range(2):
+        for i in [srv.submit(*pool[k]) for k in range(len(pool))]:
+            srv.wait(i)
     sweep = []
     for rate in [float(r) for r in args.rates.split(",")]:
         srv.reset_stats()
@@ -520,7 +573,7 @@ def bench_serve(args, rank, world, local_rank):
     return {
         "metric": "served mixed 2D/3D stream: sustained Gpx/s with p50/p99 latency (Poisson sweep)",
         "value": best["throughput_gpx_s"], "unit": "Gpx/s", "n_gpus": world, "steps": len(sweep),
-        "warmup": 4, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "warmup": 4 + 2 * len(pool), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
         "config": {"workload": "serve", "mix": "80% 2D side 256-8192, 20% 3D side 64-384 (GRF 60th pct)",
                    "pool": len(pool), "lanes": 2, "max_batch": 64, "host_buffers": "pinned"},
