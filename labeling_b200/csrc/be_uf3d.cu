@@ -646,6 +646,8 @@ __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Wo
     __shared__ uint8_t nbf[NPF];          // its face bits
     __shared__ uint2 gq[kGQ3];
     __shared__ uint32_t nq;
+    __shared__ uint32_t pl[kT3MergeThreads * 9];   // one round's listed pairs: (node << 16) | staged
+    __shared__ uint32_t npl;
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
         const Img3D im = L.get(t);
@@ -694,38 +696,59 @@ __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Wo
         for (int e = threadIdx.x; e < NPF; e += kT3MergeThreads)
             if (nbid[e] != kNone) sflatten(lp, uint32_t(MAXB + e));
         __syncthreads();
-        // Pairs: a pair whose two elements are already one local set is implied by pairs queued
-        // before it (smerge_joined); the rest are unioned globally after the loop.
-        for (int p = threadIdx.x; p < NPLUS; p += kT3MergeThreads) {
-            int u = 0, v = 0, ebase, pitch;
-            uint32_t A;
+        // Pairs: each round, the face positions of one CTA-width list their connected neighbours
+        // (a bit test each), then all lanes check the listed pairs; a pair whose two elements are
+        // already one local set is implied by pairs queued before it (smerge_joined).  The rest
+        // are unioned globally after the rounds.
+        for (int base = 0; base < NPLUS; base += kT3MergeThreads) {
+            const int p = base + int(threadIdx.x);
+            int u = 0, v = 0, ebase = 0, pitch = 1;
+            uint32_t A = 0;
             if (p < FaceAx<0>::NPOS) {
                 A = plus_entry<0>(im, g, w, t, p, u, v);
                 ebase = FaceAx<0>::EBASE; pitch = FaceAx<0>::PITCH;
             } else if (p < FaceAx<0>::NPOS + FaceAx<1>::NPOS) {
                 A = plus_entry<1>(im, g, w, t, p - FaceAx<1>::PBASE, u, v);
                 ebase = FaceAx<1>::EBASE; pitch = FaceAx<1>::PITCH;
-            } else {
+            } else if (p < NPLUS) {
                 A = plus_entry<2>(im, g, w, t, p - FaceAx<2>::PBASE, u, v);
                 ebase = FaceAx<2>::EBASE; pitch = FaceAx<2>::PITCH;
             }
-            if (!A || !GUARD(w, (A >> 4) < w.nb[t] && (A >> 4) < uint32_t(MAXB), 204, (uint64_t(t) << 16) | (A >> 4)))
-                continue;
-            const uint32_t fa = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
+            if (A && !GUARD(w, (A >> 4) < w.nb[t] && (A >> 4) < uint32_t(MAXB), 204, (uint64_t(t) << 16) | (A >> 4)))
+                A = 0;
+            const uint32_t fa = A & 15u, ja = A >> 4;
+            uint32_t hit = 0;   // bit 3 * (da + 1) + (db + 1): connected neighbour
+            if (A) {
 #pragma unroll
-            for (int da = -1; da <= 1; ++da) {
+                for (int da = -1; da <= 1; ++da) {
 #pragma unroll
-                for (int db = -1; db <= 1; ++db) {
-                    if (!(fa & face_sel(da, db))) continue;
-                    const int e = ebase + (u + 1 + da) * pitch + (v + 1 + db);
-                    const uint32_t id = nbid[e];
-                    if (id == kNone || !(nbf[e] & face_sel(-da, -db))) continue;
-                    if (!smerge_joined(lp, ja, uint32_t(MAXB + e))) continue;
-                    const uint32_t slot = atomicAdd(&nq, 1u);
-                    if (slot < uint32_t(kGQ3)) gq[slot] = make_uint2(nA, id);
-                    else gunion3d(im, w, nA, id);
+                    for (int db = -1; db <= 1; ++db) {
+                        if (!(fa & face_sel(da, db))) continue;
+                        const int e = ebase + (u + 1 + da) * pitch + (v + 1 + db);
+                        if (nbid[e] != kNone && (nbf[e] & face_sel(-da, -db))) hit |= 1u << (3 * (da + 1) + (db + 1));
+                    }
                 }
             }
+            if (threadIdx.x == 0) npl = 0;
+            __syncthreads();
+            uint32_t pos = warp_reserve(&npl, __popc(hit));
+            while (hit) {
+                const int k = __ffs(hit) - 1;
+                hit &= hit - 1;
+                const int e = ebase + (u + 1 + k / 3 - 1) * pitch + (v + 1 + k % 3 - 1);
+                pl[pos++] = (ja << 16) | uint32_t(e);
+            }
+            __syncthreads();
+            const uint32_t n = npl;
+            for (uint32_t i = threadIdx.x; i < n; i += kT3MergeThreads) {
+                const uint32_t ja2 = pl[i] >> 16, e = pl[i] & 0xFFFFu;
+                if (!smerge_joined(lp, ja2, uint32_t(MAXB) + e)) continue;
+                const uint32_t nA = uint32_t(t * MAXB + ja2), id = nbid[e];
+                const uint32_t slot = atomicAdd(&nq, 1u);
+                if (slot < uint32_t(kGQ3)) gq[slot] = make_uint2(nA, id);
+                else gunion3d(im, w, nA, id);
+            }
+            __syncthreads();
         }
         __syncthreads();
         const uint32_t nqt = min(nq, uint32_t(kGQ3));
