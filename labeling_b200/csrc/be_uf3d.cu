@@ -407,12 +407,26 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
         }
 
         // Phase C: every run start points straight at its root; roots mark their first voxel.
+        // The starts are listed (16-bit, in the free merge queue) and taken round robin, so the
+        // work is even over the lanes and a row's parents are mostly compressed already.
+        if (tid == 0) mqn[0] = 0;
+        __syncthreads();
+        uint16_t *runs = reinterpret_cast<uint16_t *>(MQ);
+        static_assert(2 * MQ1 >= NBLK, "the run list must hold every block");
         {
+            uint32_t pos = warp_reserve(&mqn[0], __popc(S));
             uint32_t ss = S;
             while (ss) {
                 const uint32_t s0 = __ffs(ss) - 1;
                 ss &= ss - 1;
-                const uint32_t x = rowb + s0;
+                runs[pos++] = uint16_t(rowb + s0);
+            }
+        }
+        __syncthreads();
+        {
+            const uint32_t nruns = mqn[0];
+            for (uint32_t i = tid; i < nruns; i += NT1) {
+                const uint32_t x = runs[i];
                 const uint32_t root = efind3_ro(P, x);
                 const uint32_t ev = P[root];
                 for (uint32_t y = x; y != root;) {
