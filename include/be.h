@@ -204,6 +204,32 @@ int be_server_destroy(be_server *server);
 int be_label2d_noalloc(const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols, int threshold,
                        int32_t *out, int64_t out_pitch, int64_t *n_components, void *stream);
 
+/* ---- Ingest and egress on the device (the steps either side of the labeling path) ---------------
+ * be_to_gray replaces ILabeling::RGB2Gray (Labeling2015/src/LabelingTools.cpp:39-49): channels 1
+ * (gray) or 3 (RGB order, cv::COLOR_RGB2GRAY: Y = (4899 R + 9617 G + 1868 B + 2^13) >> 14), then
+ * with binarize != 0 the reference's fixed threshold, Y > 8 ? 255 : 0.  Pitches in bytes. */
+int be_to_gray(be_ctx *ctx, const uint8_t *in, int64_t in_pitch, int channels, int32_t rows, int32_t cols,
+               int binarize, uint8_t *out, int64_t out_pitch, void *stream);
+
+/* be_stack_slices replaces the slice stacking of Read3DImage (Labeling2015/main.cpp:172-212):
+ * `planes` slices of rows x cols pixels (channels 1 or 3, packed slice after slice) become the
+ * volume [rows][cols][planes] -- the slice index is the fastest dimension, as the reference
+ * stacks them -- each voxel binarized as RGB2Gray does (0 / 255).  rows <= 65535. */
+int be_stack_slices(be_ctx *ctx, const uint8_t *slices, int channels, int32_t rows, int32_t cols,
+                    int32_t planes, uint8_t *volume, void *stream);
+
+/* be_labels_to_rgb replaces LabelsToRGB (Labeling2015/main.cpp:248-286): 3 bytes per label, the
+ * background black, every other label a colour hashed from (label, seed).  The reference draws
+ * its colours with std::rand in label order, so its colours are not reproducible; this map is
+ * deterministic and needs no table.  n labels in, 3 n bytes out. */
+int be_labels_to_rgb(be_ctx *ctx, const int32_t *labels, int64_t n, uint32_t seed, uint8_t *rgb, void *stream);
+
+/* be_volume_to_rgb_planes replaces the plane loop of Write3DLabels (Labeling2015/main.cpp:290-305):
+ * the label volume [d0][d1][d2] becomes d2 colour planes of d0 x d1 RGB pixels, plane after plane,
+ * coloured as be_labels_to_rgb.  d0 <= 65535. */
+int be_volume_to_rgb_planes(be_ctx *ctx, const int32_t *labels, int32_t d0, int32_t d1, int32_t d2, uint32_t seed,
+                            uint8_t *rgb, void *stream);
+
 /* Report of the bounds-checked debug build (-DBE_BOUNDS_CHECK; no counterpart in the
  * reference): out3 = {site, value low, value high} of the first failed index check of the last
  * 2D (dims = 2) or 3D (dims = 3) union-find call, all zero when none failed.  Normal builds

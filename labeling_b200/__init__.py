@@ -116,6 +116,10 @@ def lib() -> ctypes.CDLL:
     l.be_set_stage_timing.argtypes = [vp, c_int]
     l.be_check_status.argtypes = [vp, c_int, ctypes.POINTER(ctypes.c_uint32)]
     l.be_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), c_int, ctypes.POINTER(c_int)]
+    l.be_to_gray.argtypes = [vp, vp, i64, c_int, i32, i32, c_int, vp, i64, vp]
+    l.be_stack_slices.argtypes = [vp, vp, c_int, i32, i32, i32, vp, vp]
+    l.be_labels_to_rgb.argtypes = [vp, vp, i64, ctypes.c_uint32, vp, vp]
+    l.be_volume_to_rgb_planes.argtypes = [vp, vp, i32, i32, i32, ctypes.c_uint32, vp, vp]
     _lib = l
     return l
 
@@ -228,6 +232,44 @@ def label3d(ctx: Context, vol, out, threshold: int = 0, algo: int = ALGO_AUTO,
     ctx.check(lib().be_label3d(ctx.handle, _ptr(vol), d0, d1, d2, threshold, algo, _ptr(out),
                                ctypes.byref(n) if want_count else None, _stream(stream)))
     return int(n.value) if want_count else None
+
+
+# ---- ingest and egress on the device (RGB2Gray, Read3DImage, LabelsToRGB, Write3DLabels) -----
+
+def to_gray(ctx: Context, img, out, binarize: bool = True, stream=None) -> None:
+    """uint8 CUDA tensor [rows, cols] or [rows, cols, 3] (RGB) -> uint8 [rows, cols]: gray as
+    cv::COLOR_RGB2GRAY, then (binarize) the reference's fixed threshold, gray > 8 ? 255 : 0."""
+    channels = int(img.shape[2]) if img.dim() == 3 else 1
+    rows, cols = int(img.shape[0]), int(img.shape[1])
+    ctx.check(lib().be_to_gray(ctx.handle, _ptr(img), int(img.stride(0)), channels, rows, cols,
+                               int(bool(binarize)), _ptr(out), int(out.stride(0)), _stream(stream)))
+
+
+def stack_slices(ctx: Context, slices, out, stream=None) -> None:
+    """Contiguous uint8 CUDA tensor of slices [planes, rows, cols] (or [..., 3] RGB) -> binarized
+    volume ``out`` [rows, cols, planes], the slice index fastest (Read3DImage's layout)."""
+    channels = int(slices.shape[3]) if slices.dim() == 4 else 1
+    planes, rows, cols = (int(x) for x in slices.shape[:3])
+    assert slices.is_contiguous() and out.is_contiguous() and tuple(out.shape) == (rows, cols, planes)
+    ctx.check(lib().be_stack_slices(ctx.handle, _ptr(slices), channels, rows, cols, planes, _ptr(out),
+                                    _stream(stream)))
+
+
+def labels_to_rgb(ctx: Context, labels, out, seed: int = 0, stream=None) -> None:
+    """Contiguous int32 labels (any shape) -> uint8 ``out`` of shape labels.shape + (3,): the
+    background black, every label a colour hashed from (label, seed)."""
+    assert labels.is_contiguous() and out.is_contiguous() and out.numel() == 3 * labels.numel()
+    ctx.check(lib().be_labels_to_rgb(ctx.handle, _ptr(labels), int(labels.numel()), seed & 0xFFFFFFFF,
+                                     _ptr(out), _stream(stream)))
+
+
+def volume_to_rgb_planes(ctx: Context, labels, out, seed: int = 0, stream=None) -> None:
+    """int32 label volume [d0, d1, d2] -> uint8 ``out`` [d2, d0, d1, 3]: one colour image per index
+    of the last dimension (Write3DLabels's planes)."""
+    d0, d1, d2 = (int(x) for x in labels.shape)
+    assert labels.is_contiguous() and out.is_contiguous() and tuple(out.shape) == (d2, d0, d1, 3)
+    ctx.check(lib().be_volume_to_rgb_planes(ctx.handle, _ptr(labels), d0, d1, d2, seed & 0xFFFFFFFF,
+                                            _ptr(out), _stream(stream)))
 
 
 def label2d_host(ctx: Context, img: np.ndarray, threshold: int = 0, algo: int = ALGO_AUTO,
@@ -404,11 +446,26 @@ class Labeling:
     def Label(self, pixels: np.ndarray, threads: int = 0, coh: int = COH_DEFAULT):
         if pixels.size == 0:
             raise ValueError("Labeling.Label : Input image is empty")
-        if pixels.ndim == 3:   # colour input: cv::cvtColor(COLOR_RGB2GRAY) weights
-            pixels = np.rint(pixels[..., 0] * 0.299 + pixels[..., 1] * 0.587 +
-                             pixels[..., 2] * 0.114).astype(np.uint8)
+        if pixels.ndim == 3:   # colour input: cv::cvtColor(COLOR_RGB2GRAY), 14-bit fixed point
+            r, g, b = (pixels[..., k].astype(np.uint32) for k in range(3))
+            pixels = ((r * 4899 + g * 9617 + b * 1868 + (1 << 13)) >> 14).astype(np.uint8)
         labels, _, us = label2d_host(self.ctx, pixels, self.threshold, self.algo, coh)
         return labels, us
+
+
+class RunEquivalence(Labeling):
+    """The ``runeq -g`` slot (TOCLRunEquivLabeling, LabelingAlgs.cpp:1090-1268): the reference's
+    run kernels join runs that overlap in a column -- 4-connectivity -- whatever coherence is
+    asked for, and reject COH_4 themselves; so does this: COH_4 raises, anything else labels
+    4-connected on the pixel-level path."""
+
+    def __init__(self, device: int = 0):
+        super().__init__(ALGO_PIXEL, device)
+
+    def Label(self, pixels: np.ndarray, threads: int = 0, coh: int = COH_DEFAULT):
+        if coh == COH_4:
+            raise ValueError("RunEquivalence.Label : 4x connectivity is not implemented for this method")
+        return super().Label(pixels, threads, COH_4)
 
 
 class Labeling3D:
@@ -436,6 +493,7 @@ class Labeling3D:
 ALGORITHMS = {
     "bleq": ("Block equivalence by Zavalishin et.al. 2016", ALGO_AUTO),
     "lbeq": ("Label equivalence by Kalentev et.al. 2012 (pixel level)", ALGO_PIXEL),
+    "runeq": ("Run equivalence by Bekhtin et.al. 2015 (4-connected, 2D only)", ALGO_PIXEL),
 }
 
 
@@ -448,4 +506,8 @@ def make_labeler(name: str, gpu: bool = True, three_d: bool = False, device: int
     if not gpu:
         raise ValueError("Chosen algorithm doesn't support specified capabilities (CPU mode)")
     algo = ALGORITHMS[name][1]
+    if name == "runeq":
+        if three_d:   # the reference has no 3D run equivalence (main.cpp:127-130)
+            raise ValueError("Chosen algorithm doesn't support specified capabilities (3D)")
+        return RunEquivalence(device)
     return Labeling3D(algo, device) if three_d else Labeling(algo, device)

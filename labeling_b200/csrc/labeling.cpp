@@ -92,6 +92,15 @@ TTime TCudaBlockEquivalence3D::Label(const TImage &pixels, TLabelImage &labels, 
     return TTime(us);
 }
 
+TCudaRunEquivalence::TCudaRunEquivalence(bool runOnGPU, int device) : inner_(runOnGPU, BE_ALGO_PIXEL, device) {}
+
+TTime TCudaRunEquivalence::Label(const TImage &pixels, TLabelImage &labels, char threads, TCoherence coh)
+{
+    if (coh == COH_4)   // as TOCLRunEquivLabeling::DoOCLLabel (LabelingAlgs.cpp:1229)
+        throw Error(BE_ERR_INVALID, "TCudaRunEquivalence::Label : 4x connectivity is not implemented for this method");
+    return inner_.Label(pixels, labels, threads, COH_4);
+}
+
 const std::map<std::string, Algs> &AlgList()
 {
     static const std::map<std::string, Algs> list = {
@@ -103,6 +112,9 @@ const std::map<std::string, Algs> &AlgList()
          {"Label equivalence by Kalentev et.al. 2012 (pixel level, B200)", nullptr,
           [](bool gpu) { return std::make_shared<TCudaBlockEquivalence>(gpu, BE_ALGO_PIXEL); }, nullptr,
           [](bool gpu) { return std::make_shared<TCudaBlockEquivalence3D>(gpu, BE_ALGO_PIXEL); }}},
+        {"runeq",
+         {"Run equivalence by Bekhtin et.al. 2015 (4-connected, B200)", nullptr,
+          [](bool gpu) { return std::make_shared<TCudaRunEquivalence>(gpu); }, nullptr, nullptr}},
     };
     return list;
 }

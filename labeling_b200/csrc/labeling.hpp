@@ -88,6 +88,20 @@ private:
     int algo_;
 };
 
+// GPU run equivalence, 2D (the `runeq` GPU slot; replaces TOCLRunEquivLabeling,
+// LabelingAlgs.cpp:1090-1268).  The reference's run kernels join runs that overlap in a column,
+// which is 4-connectivity, whatever coherence is asked for, and it rejects COH_4 itself; this
+// slot keeps both: COH_4 throws, anything else labels 4-connected, on the pixel-level path.
+class TCudaRunEquivalence final : public ILabeling {
+public:
+    explicit TCudaRunEquivalence(bool runOnGPU = true, int device = 0);
+    TTime Label(const TImage &pixels, TLabelImage &labels, char threads = MAX_THREADS,
+                TCoherence coh = COH_DEFAULT) override;
+
+private:
+    TCudaBlockEquivalence inner_;
+};
+
 // The algorithm registry of the reference's demo (main.cpp:88-131) for the slots this library
 // fills.  CPU slots stay empty: there is no CPU fallback.
 struct Algs {

@@ -63,6 +63,7 @@ def ref_lib() -> Optional[ctypes.CDLL]:
         l.ref_lbeq3d_raw.argtypes = [_u8p, _long, _long, _long, ctypes.c_int, _u32p]
         l.ref_bleq3d_timed.argtypes = [_u8p, _long, _long, _long, ctypes.c_int, _u32p,
                                        ctypes.POINTER(ctypes.c_double)]
+        l.ref_runeq2d_raw.argtypes = [_u8p, _long, _long, _long, ctypes.c_int, _u32p]
         l.ref_set_threads.argtypes = [ctypes.c_int]
         l.ref_set_threads.restype = ctypes.c_int
     return l
@@ -225,6 +226,19 @@ def ref_distr2d_raw(img: np.ndarray, thr: int = 0, coh: int = 2) -> np.ndarray:
     if l.ref_distr2d_raw(_p(img, _u8p), img.shape[0], img.shape[1], img.shape[1], thr, coh,
                          _p(out, _u32p)):
         raise RuntimeError("ref_distr2d_raw failed")
+    return out
+
+
+def ref_runeq2d_raw(img: np.ndarray, thr: int = 0) -> np.ndarray:
+    """The reference's GPU run-equivalence kernels (RE*, LabelingAlgs.cl:325-616) with its host
+    flow (TOCLRunEquivLabeling, LabelingAlgs.cpp:1090-1268), serially on the host."""
+    l = ref_lib()
+    if l is None:
+        raise RuntimeError("oracle/_ref/libref_be.so is not built")
+    img = _u8(img)
+    out = np.empty(img.shape, np.uint32)
+    if l.ref_runeq2d_raw(_p(img, _u8p), img.shape[0], img.shape[1], img.shape[1], thr, _p(out, _u32p)):
+        raise RuntimeError("ref_runeq2d_raw failed")
     return out
 
 

@@ -149,6 +149,34 @@ int ref_distr2d_raw(const uint8_t *img, long rows, long cols, long pitch, int th
     return 0;
 }
 
+// TOCLRunEquivLabeling::DoOCLLabel (LabelingAlgs.cpp:1226-1268): REInitRuns, REFindRuns,
+// REFindNeib, then REScan / REAnalize until no change, RELabel -- one work-item per row of the
+// IOCLLabeling::Label padded image; the labels are cropped to rows x cols.
+int ref_runeq2d_raw(const uint8_t *img, long rows, long cols, long pitch, int thr, uint32_t *out)
+{
+    if (rows <= 0 || cols <= 0) return -1;
+    const long W = (cols >> 5 << 5) + 32, H = (rows >> 5 << 5) + 32;
+    std::vector<uchar> pix = pad2d(img, rows, cols, pitch, thr, W, H);
+    std::vector<TLabel> labels((size_t)W * H, 0);
+    std::vector<TRun> runs((size_t)H * (W >> 1));
+    std::memset(runs.data(), 0, runs.size() * sizeof(TRun));
+    std::vector<uint> runNum((size_t)H, 0);
+    const size_t n[1] = {(size_t)H};
+    ref_ndrange(1, n, [&] { REInitRunsKernel(runNum.data()); });
+    ref_ndrange(1, n, [&] { REFindRunsKernel(pix.data(), runs.data(), runNum.data(), (uint)W); });
+    ref_ndrange(1, n, [&] { REFindNeibKernel(runs.data(), runNum.data(), (uint)W); });
+    for (;;) {
+        char noChanges = 1;
+        ref_ndrange(1, n, [&] { REScanKernel(runs.data(), runNum.data(), (uint)W, &noChanges); });
+        if (noChanges) break;
+        ref_ndrange(1, n, [&] { REAnalizeKernel(runs.data(), runNum.data(), (uint)W); });
+    }
+    ref_ndrange(1, n, [&] { RELabelKernel(runs.data(), runNum.data(), labels.data(), (uint)W); });
+    for (long y = 0; y < rows; ++y)
+        std::memcpy(out + y * cols, labels.data() + (size_t)y * W, sizeof(uint32_t) * cols);
+    return 0;
+}
+
 // TOCLLabelEquivalence3D::DoOCLLabel3D (LabelingAlgs.cpp:1362-1396) on the CopyAlignImg volume.
 int ref_lbeq3d_raw(const uint8_t *vol, long d0, long d1, long d2, int thr, uint32_t *out)
 {

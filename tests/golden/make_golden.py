@@ -68,6 +68,7 @@ def main():
         assert O.canon(g.astype(np.uint32))[1] == k == kg, name
         d4 = O.ref_distr2d_raw(img, thr, 2)              # reference -a lbeq -g (COH_DEFAULT)
         d8 = O.ref_distr2d_raw(img, thr, 1)              # reference -a lbeq -g -c 8
+        re = O.ref_runeq2d_raw(img, thr)                 # reference -a runeq -g (RE* kernels)
         data[f"2d/{name}/img"] = img
         data[f"2d/{name}/thr"] = np.array(thr)
         data[f"2d/{name}/raw"] = raw
@@ -76,6 +77,7 @@ def main():
         data[f"2d/{name}/grana"] = g
         data[f"2d/{name}/distr4"] = d4
         data[f"2d/{name}/distr8"] = d8
+        data[f"2d/{name}/runeq"] = re
     for name, vol in cases_3d(rng):
         raw = O.ref_be3d_raw(vol, 0)                     # reference BLEQ3D_* label values
         can, k = O.canon(raw)

@@ -142,3 +142,23 @@ def test_pixel_label_equivalence_lbeq(ctx, golden, conn8):
         lab, n, _ = be.label2d_host(ctx, img, 0, be.ALGO_PIXEL, coh)
         ref, k = O.ccl2d(img, 0, conn8=conn8)
         assert n == k and np.array_equal(lab, ref)
+
+
+def test_run_equivalence_slot_matches_reference_kernels(ctx, golden):
+    """-a runeq -g: the reference's run kernels (golden outputs) give 4-connected components; the
+    slot labels them on the pixel path with 4-connectivity and rejects COH_4 as the reference."""
+    import labeling_b200 as be
+    for (dim, name), c in golden.items():
+        if dim != "2d":
+            continue
+        lab, n, _ = be.label2d_host(ctx, c["img"], int(c["thr"]), be.ALGO_PIXEL, be.COH_4)
+        want, k = O.canon(c["runeq"])
+        assert n == k and np.array_equal(lab, want), name
+    lab_alg = be.make_labeler("runeq")
+    img = (np.random.default_rng(4).random((90, 130)) < 0.5).astype(np.uint8) * 255
+    labels, _ = lab_alg.Label(img)
+    assert np.array_equal(labels, O.ccl2d(img, 8, False)[0])
+    with pytest.raises(ValueError):
+        lab_alg.Label(img, coh=be.COH_4)
+    with pytest.raises(ValueError):
+        be.make_labeler("runeq", three_d=True)

@@ -109,11 +109,15 @@ def test_reference_cpu_bleq_matches_oracle_with_one_background_row_and_column(se
 def test_reference_cpu_bleq_right_border_wrap_is_the_references():
     """At the right border the reference's CPU block labeler reads the next row's first pixels
     (RemoveBorderBlocks compares pixel coordinates with the image size, LabelingAlgs.cpp:366-374):
-    in this 4 x 2 image the two components come out as one.  The GPU path follows the reference's
-    GPU kernels, which pad the image and do not wrap."""
-    img = np.array([[1, 0], [0, 0], [1, 1], [1, 0]], np.uint8) * 255
+    in this 4 x 4 image the pixel at (0, 3) "touches" (1, 0) through the wrap, and the two
+    components come out as one.  With the background row and column the baseline appends, the
+    labels are exact.  The GPU path follows the reference's GPU kernels, which pad the image and
+    do not wrap."""
+    img = np.zeros((4, 4), np.uint8)
+    img[0, 3] = img[1, 0] = img[2, 0] = 255
     raw, _ = O.ref_cpu_bleq(img, pad=False)
     assert O.canon(raw)[1] == 1 and O.ccl2d(img)[1] == 2
+    assert O.canon(O.ref_cpu_bleq(img)[0])[1] == 2
 
 
 @needs_ref_kernels
@@ -127,3 +131,13 @@ def test_reference_3d_kernels_threaded_match_serial():
         threaded, _ = O.ref_be3d_timed(vol, 0, 0)
         ref = O.ccl3d(vol)[0]
         assert np.array_equal(O.canon(serial)[0], ref) and np.array_equal(O.canon(threaded)[0], ref)
+
+
+def test_reference_run_equivalence_kernels_are_4_connected(golden):
+    """The reference's GPU run equivalence (RE* kernels, golden outputs) joins runs that overlap in
+    a column: its labels are exactly the 4-connected components, which is what the runeq slot of
+    this package returns."""
+    for (dim, name), c in golden.items():
+        if dim != "2d":
+            continue
+        assert np.array_equal(O.canon(c["runeq"])[0], O.ccl2d(c["img"], int(c["thr"]), False)[0]), name
