@@ -9,7 +9,7 @@ constexpr int NPERIM = 2 * (TBW + TBH);            // border positions per tile
 constexpr int MAXB = NPERIM;                       // nodes per tile
 constexpr int WPR = TBW / 32;                      // 32-block words per block row
 constexpr int K1_NT = TBH * WPR;                   // one thread per (block row, word) = NBLK / 32
-constexpr int MQCAP = NBLK;                        // merge-queue capacity (links per tile)
+constexpr int MQCAP = 2816;                        // merge-queue capacity (more merge in place)
 constexpr uint32_t kPass = 0xFFFFu;                // "no run start" in the carry scan
 
 static_assert(NBLK <= 4096, "tile-local block index must fit 12 bits");
@@ -124,7 +124,7 @@ __device__ __forceinline__ void eunion(uint32_t *P, uint32_t a, uint32_t b)
 // operations; only runs enter the union-find, and only links between runs that no earlier link
 // already joins are merged.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(K1_NT, 5) k_tile_local_2d(ImgList2D L, Work w)
+__global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
 {
     __shared__ uint32_t P[NBLK];            // run starts: (slot << 12) | parent
     __shared__ __align__(16) uint8_t M[NBLK];
@@ -351,6 +351,9 @@ __global__ void __launch_bounds__(K1_NT, 5) k_tile_local_2d(ImgList2D L, Work w)
         // The starts are listed first (the merge queue is free again) and taken round robin, so
         // the work is even over the lanes and a row's parents -- the row above, listed one
         // round earlier -- are mostly already compressed when a row is walked.
+        // The list is 16-bit (block indices) in the queue's memory: it holds every block.
+        static_assert(2 * MQCAP >= NBLK, "the run list must hold every block of a tile");
+        uint16_t *runs = reinterpret_cast<uint16_t *>(MQ);
         if (tid == 0) mqn = 0;
         __syncthreads();
         {
@@ -359,14 +362,14 @@ __global__ void __launch_bounds__(K1_NT, 5) k_tile_local_2d(ImgList2D L, Work w)
             while (ss) {
                 const uint32_t s0 = __ffs(ss) - 1;
                 ss &= ss - 1;
-                MQ[pos++] = rbase + 32 * q + s0;
+                runs[pos++] = uint16_t(rbase + 32 * q + s0);
             }
         }
         __syncthreads();
         {
             const uint32_t nruns = mqn;
             for (uint32_t i = tid; i < nruns; i += K1_NT) {
-                const uint32_t x = MQ[i];
+                const uint32_t x = runs[i];
                 const uint32_t root = efind_ro(P, x);
                 const uint32_t ev = P[root];
                 // Point the whole path at the root (every writer stores the same final value).
@@ -816,7 +819,7 @@ inline cudaError_t launch(const ImgList2D &L, const Work &w, int sms, bool persi
     Work wk = w;
     if (!persistent) wk.queue = nullptr;
     mark(0);
-    k_tile_local_2d<<<grid(w.n_tiles, 5), K1_NT, 0, s>>>(L, wk);
+    k_tile_local_2d<<<grid(w.n_tiles, 6), K1_NT, 0, s>>>(L, wk);
     mark(1);
     k_merge_2d<<<grid(w.n_tiles, 8), K2_NT, 0, s>>>(L, wk);
     mark(2);
