@@ -266,12 +266,10 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
         // and NE (top-right to the bottom-left pixel of b + 1 above).  A link is dropped when an
         // earlier link (further left, or N before NW / NE at the same block) joins the same two
         // runs; every chain of such reasons ends at a link that is kept.
-        uint32_t Nm = 0, NWm = 0, NEm = 0, uS = 0, uCS = 0;
+        uint32_t Nm = 0, NWm = 0, NEm = 0;
         if (r > 0 && r < nbr) {
             const int u = tid - WPR;   // same word, row above
             const uint32_t uBL = WBL[u], uBR = WBR[u], uhc = WHC[u];
-            uS = WS[u];
-            uCS = WCS[u];
             const uint32_t uBRp = q > 0 ? WBR[u - 1] >> 31 : 0u;
             const uint32_t uBLn = q + 1 < WPR ? WBL[u + 1] & 1u : 0u;
             const uint32_t uhl = (uhc << 1) | (q > 0 ? WHC[u - 1] >> 31 : 0u);
@@ -298,22 +296,22 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
         }
         const uint32_t n = __popc(Nm) + __popc(NWm) + __popc(NEm);
         uint32_t pos = warp_reserve(&mqn, n);
+        // The queue holds the two blocks of each link; their run starts (a start in the block's
+        // word at or before it, else the start carried in from the left) are looked up by the
+        // merging lanes, which share that work evenly.
+        auto start_of = [&](uint32_t blk) -> uint32_t {
+            const uint32_t m = WS[blk >> 5] & ((2u << (blk & 31u)) - 1u);
+            const uint32_t st = m ? (blk & ~31u) + hibit(m) : (blk & ~uint32_t(TBW - 1)) + WCS[blk >> 5];
+            // A start of this tile by construction; the mask only keeps a broken invariant
+            // from leaving the array.
+            GUARD(w, st < uint32_t(NBLK), 112, (uint64_t(blk) << 32) | st);
+            return st & (NBLK - 1);
+        };
         {
-            const uint32_t ubase = rbase - TBW;
-            // Start column of the run holding block column c (in this word, c in [0, 31]) of a
-            // row with run starts S_ and carried start CS_.
-            auto start_in = [&](uint32_t S_, uint32_t CS_, uint32_t c) -> uint32_t {
-                const uint32_t m = S_ & ((2u << c) - 1u);
-                return m ? uint32_t(32 * q) + hibit(m) : CS_;
-            };
+            const uint32_t ubase = rbase - TBW + 32 * q, abase = rbase + 32 * q;
             auto push = [&](uint32_t a, uint32_t b) {
-                // Both are run starts of this tile by construction; the mask only keeps a
-                // broken invariant from leaving the array.
-                GUARD(w, a < uint32_t(NBLK) && b < uint32_t(NBLK), 112, (uint64_t(a) << 32) | b);
-                a &= NBLK - 1;
-                b &= NBLK - 1;
                 if (pos < uint32_t(MQCAP)) MQ[pos] = (a << 16) | b;
-                else eunion(P, a, b);   // queue full: merge in place
+                else eunion(P, start_of(a), start_of(b));   // queue full: merge in place
                 ++pos;
             };
             uint32_t todo = Nm | NWm | NEm;
@@ -321,29 +319,16 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
                 const uint32_t b = __ffs(todo) - 1;
                 todo &= todo - 1;
                 const uint32_t bit = 1u << b;
-                const uint32_t a = rbase + start_in(S, CSc, b);
-                if (Nm & bit) push(a, ubase + start_in(uS, uCS, b));
-                if (NWm & bit) {
-                    uint32_t c;
-                    if (b > 0) c = start_in(uS, uCS, b - 1);
-                    else {
-                        const uint32_t pS = WS[tid - WPR - 1];
-                        c = pS ? uint32_t(32 * (q - 1)) + hibit(pS) : WCS[tid - WPR - 1];
-                    }
-                    push(a, ubase + c);
-                }
-                if (NEm & bit) {
-                    uint32_t c;
-                    if (b < 31) c = start_in(uS, uCS, b + 1);
-                    else c = (WS[tid - WPR + 1] & 1u) ? uint32_t(32 * (q + 1)) : WCS[tid - WPR + 1];
-                    push(a, ubase + c);
-                }
+                const uint32_t a = abase + b;
+                if (Nm & bit) push(a, ubase + b);
+                if (NWm & bit) push(a, ubase + b - 1);   // b = 0: the last block of the word before
+                if (NEm & bit) push(a, ubase + b + 1);   // b = 31: the first block of the word after
             }
         }
         __syncthreads();
         {
             const uint32_t nq = min(mqn, uint32_t(MQCAP));
-            for (uint32_t i = tid; i < nq; i += K1_NT) eunion(P, MQ[i] >> 16, MQ[i] & 0xFFFFu);
+            for (uint32_t i = tid; i < nq; i += K1_NT) eunion(P, start_of(MQ[i] >> 16), start_of(MQ[i] & 0xFFFFu));
         }
         __syncthreads();
 

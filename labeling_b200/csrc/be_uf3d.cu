@@ -72,17 +72,15 @@ __device__ __forceinline__ int face_base(int f)
 // The four voxels of a block on face f, as bits (a*2 + b) over the two tangent axes in order.
 __device__ __forceinline__ uint32_t face_bits(uint32_t m, int f)
 {
-    const int axis = f >> 1, off = f & 1;
-    uint32_t r = 0;
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-        const int i = v >> 2, j = (v >> 1) & 1, k = v & 1;
-        const int o = axis == 0 ? i : axis == 1 ? j : k;
-        if (o != off || !((m >> v) & 1u)) continue;
-        const int ta = axis == 0 ? j : i, tb = axis == 2 ? j : k;
-        r |= 1u << (ta * 2 + tb);
+    // Mask bit v = 4i + 2j + k; the face's four voxels in the order (first tangent, second).
+    const uint32_t s = uint32_t(f & 1);
+    switch (f >> 1) {
+    case 0: return (m >> (4 * s)) & 0xFu;                                          // (j, k)
+    case 1: return ((m >> (2 * s)) & 3u) | (((m >> (4 + 2 * s)) & 3u) << 2);       // (i, k)
+    default:                                                                        // (i, j)
+        return ((m >> s) & 1u) | (((m >> (2 + s)) & 1u) << 1) | (((m >> (4 + s)) & 1u) << 2) |
+               (((m >> (6 + s)) & 1u) << 3);
     }
-    return r;
 }
 
 // Selector over face bits (a*2 + b) for the tangent offsets (da, db).
@@ -116,9 +114,11 @@ __device__ __forceinline__ TileGeo tile_geo(const Img3D &im, int64_t t)
 // Block position of border position p (face f, index q), when valid for this tile.
 __device__ __forceinline__ bool perim_pos3(int p, const TileGeo &g, int &f, int &b0, int &b1, int &b2)
 {
-    f = 0;
-    int q = p;
-    while (f < 5 && q >= face_base(f + 1) - face_base(f)) { q -= face_base(f + 1) - face_base(f); ++f; }
+    constexpr int F0 = TB1 * TB2, F1 = TB0 * TB2;   // positions on a d0 face, on a d1 face
+    int q;
+    if (p < 2 * F0) { f = p >= F0; q = p - f * F0; }
+    else if (p < 2 * F0 + 2 * F1) { const int r = p - 2 * F0; f = 2 + (r >= F1); q = r - (f - 2) * F1; }
+    else { const int r = p - 2 * F0 - 2 * F1; f = 4 + (r >= TB0 * TB1); q = r - (f - 4) * TB0 * TB1; }
     const int axis = f >> 1, hi = f & 1;
     if (axis == 0) { b0 = hi ? g.n0 - 1 : 0; b1 = q / TB2; b2 = q % TB2; }
     else if (axis == 1) { b1 = hi ? g.n1 - 1 : 0; b0 = q / TB2; b2 = q % TB2; }
@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
         for (int nr = 0; nr < 4; ++nr) {
             const int dx = nr < 3 ? -1 : 0, dy = nr < 3 ? nr - 1 : -1;
             const int r0 = b0 + dx, r1 = b1 + dy;
-            uint32_t N = 0, NW = 0, NE = 0, uS = 0;
+            uint32_t N = 0, NW = 0, NE = 0;
             int ur = 0;
             if (Fw && r0 >= 0 && r1 >= 0 && r1 < TB1) {
                 ur = r0 * TB1 + r1;
@@ -373,7 +373,6 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
                     B0 = face_word<0, 1, 0>(u); Bm = face_word<0, 1, 1>(u); Bp = face_word<0, 1, -1>(u);
                 }
                 const uint32_t uhz = WHZ[ur], uhl = uhz << 1;
-                uS = WS[ur];
                 const uint32_t n0 = A0 & B0, nw = Am & (Bm << 1), ne = Ap & (Bp >> 1);
                 const uint32_t Nsh = n0 << 1, NEsh = ne << 1;
                 N = n0 & ~(hl & ((Nsh & uhl) | NEsh));
@@ -382,11 +381,16 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
             }
             const uint32_t n = __popc(N) + __popc(NW) + __popc(NE);
             uint32_t pos = warp_reserve(&mqn[nr], n);
+            // The queue holds the two blocks of each link; their run starts are looked up by the
+            // merging lanes, which share that work evenly.
+            auto start_of = [&](uint32_t b) -> uint32_t {
+                return (b & ~31u) + hibit3(WS[b >> 5] & ((2u << (b & 31u)) - 1u));
+            };
             {
                 const uint32_t ubase = uint32_t(ur) * TB2;
                 auto push = [&](uint32_t a, uint32_t b) {
                     if (pos < uint32_t(MQ1)) MQ[pos] = (a << 16) | b;
-                    else eunion3(P, a, b);   // queue full: merge in place
+                    else eunion3(P, start_of(a), start_of(b));   // queue full: merge in place
                     ++pos;
                 };
                 uint32_t todo = N | NW | NE;
@@ -394,15 +398,15 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
                     const uint32_t k = __ffs(todo) - 1;
                     todo &= todo - 1;
                     const uint32_t bit = 1u << k;
-                    const uint32_t a = rowb + hibit3(S & ((2u << k) - 1u));
-                    if (N & bit) push(a, ubase + hibit3(uS & ((2u << k) - 1u)));
-                    if (NW & bit) push(a, ubase + hibit3(uS & ((1u << k) - 1u)));
-                    if (NE & bit) push(a, ubase + hibit3(uS & ((4u << k) - 1u)));
+                    const uint32_t a = rowb + k;
+                    if (N & bit) push(a, ubase + k);
+                    if (NW & bit) push(a, ubase + k - 1);
+                    if (NE & bit) push(a, ubase + k + 1);
                 }
             }
             __syncthreads();
             const uint32_t nq = min(mqn[nr], uint32_t(MQ1));
-            for (uint32_t q = tid; q < nq; q += NT1) eunion3(P, MQ[q] >> 16, MQ[q] & 0xFFFFu);
+            for (uint32_t q = tid; q < nq; q += NT1) eunion3(P, start_of(MQ[q] >> 16), start_of(MQ[q] & 0xFFFFu));
             __syncthreads();
         }
 
