@@ -196,79 +196,6 @@ __device__ __forceinline__ void smerge(uint32_t *P, uint32_t a, uint32_t b)
     }
 }
 
-// ---- 16-bit shared-memory union-find (indices < 65536) ---------------------------------------
-// Same algorithm as sfind / smerge on uint16 parents, which halves the footprint.  The atomic
-// minimum is a compare-and-swap on the aligned 32-bit word holding the entry; plain 16-bit stores
-// to either half of that word make the CAS retry, which is all the correctness needs.
-__device__ __forceinline__ uint32_t atomic_min_u16(uint16_t *addr, uint32_t val)
-{
-    uint32_t *word = reinterpret_cast<uint32_t *>(reinterpret_cast<uintptr_t>(addr) & ~uintptr_t(3));
-    const uint32_t sh = (reinterpret_cast<uintptr_t>(addr) & 2) * 8;
-    uint32_t old = *reinterpret_cast<volatile uint32_t *>(word);
-    for (;;) {
-        const uint32_t cur = (old >> sh) & 0xFFFFu;
-        if (val >= cur) return cur;
-        const uint32_t nv = (old & ~(0xFFFFu << sh)) | (val << sh);
-        const uint32_t seen = atomicCAS(word, old, nv);
-        if (seen == old) return cur;
-        old = seen;
-    }
-}
-
-__device__ __forceinline__ uint32_t sfind16(uint16_t *P, uint32_t a)
-{
-    uint32_t p = P[a];
-    while (p != a) {
-        const uint32_t g = P[p];
-        if (g != p) P[a] = uint16_t(g);
-        a = p;
-        p = g;
-    }
-    return a;
-}
-
-__device__ __forceinline__ uint32_t sfind16_ro(const uint16_t *P, uint32_t a)
-{
-    uint32_t p = P[a];
-    while (p != a) {
-        a = p;
-        p = P[a];
-    }
-    return a;
-}
-
-// Root of `a` after all merges, pointing every entry on the path straight at it.  Safe while
-// other threads do the same: all of them store the same final root into shared entries.
-__device__ __forceinline__ uint32_t sflatten16(uint16_t *P, uint32_t a)
-{
-    const uint32_t r = sfind16_ro(P, a);
-    uint32_t x = a;
-    while (x != r) {
-        const uint32_t nx = P[x];
-        P[x] = uint16_t(r);
-        x = nx;
-    }
-    return r;
-}
-
-__device__ __forceinline__ void smerge16(uint16_t *P, uint32_t a, uint32_t b)
-{
-    for (;;) {
-        a = sfind16(P, a);
-        b = sfind16(P, b);
-        if (a == b) return;
-        if (a < b) {
-            const uint32_t old = atomic_min_u16(&P[b], a);
-            if (old == b) return;
-            b = old;
-        } else {
-            const uint32_t old = atomic_min_u16(&P[a], b);
-            if (old == a) return;
-            a = old;
-        }
-    }
-}
-
 // Appends this lane's `n` merge pairs to a shared queue with one atomic per warp; returns the
 // lane's first position (positions >= capacity mean the queue is full for those pairs).
 __device__ __forceinline__ uint32_t warp_reserve(uint32_t *count, uint32_t n)
