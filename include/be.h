@@ -230,6 +230,38 @@ int be_labels_to_rgb(be_ctx *ctx, const int32_t *labels, int64_t n, uint32_t see
 int be_volume_to_rgb_planes(be_ctx *ctx, const int32_t *labels, int32_t d0, int32_t d1, int32_t d2, uint32_t seed,
                             uint8_t *rgb, void *stream);
 
+/* ---- Slab split of one image (no counterpart in the reference, which labels one image on one
+ * device, LabelingAlgs.cpp:989-1084) ----------------------------------------------------------
+ * A slab is a band of consecutive rows of a 2D image, or of consecutive planes along d0 of a
+ * volume, labeled on its own by be_label2d / be_label3d (on its own GPU, or in turn on one GPU):
+ * its labels are 1..counts[s] in first-pixel order within the slab.  One exchange step joins the
+ * slabs: gather every slab's first and last row (plane) of labels and its count, call
+ * be_slab_merge (host only, identical on every rank), then be_slab_relabel on each slab.
+ *
+ * be_slab_merge: n_slabs slabs in image order; a border row (plane) is plane_rows x plane_cols
+ * labels (2D: plane_rows = 1, plane_cols = cols; 3D: d1 x d2).  tops / bottoms hold the slabs'
+ * first / last rows, slab after slab.  Pieces touching across a border are joined
+ * (8-connectivity across a row, 26-connectivity across a plane).  Out: offsets[s] (root pieces
+ * of the slabs before s), *n_total (components of the whole image), and per slab the ascending
+ * local labels of its pieces that were joined under an earlier piece, with their final labels:
+ * joined_labels / joined_targets[joined_start[s] .. joined_start[s + 1]).  cap = capacity of the
+ * joined arrays; 2 * plane_rows * plane_cols * n_slabs always suffices.  BE_ERR_INVALID on bad
+ * sizes, labels outside 0..counts[s], a cap too small or more than INT32_MAX components. */
+int be_slab_merge(int32_t n_slabs, int32_t plane_rows, int32_t plane_cols, const int64_t *counts,
+                  const int32_t *tops, const int32_t *bottoms, int64_t *offsets, int64_t *n_total,
+                  int32_t *joined_labels, int32_t *joined_targets, int64_t *joined_start, int64_t cap);
+
+/* be_slab_relabel: maps the local labels of one slab (device array of n_rows rows of cols labels,
+ * pitch in elements; a 3D slab of p planes is p * d1 rows of d2) to the whole image's labels:
+ * joined labels to their targets, every other label l in 1..count to offset + l - (joined labels
+ * below l).  joined_labels (ascending) / joined_targets are HOST arrays of n_joined entries, as
+ * be_slab_merge returns them for this slab; pageable memory is read before the call returns,
+ * pinned memory must stay valid until the stream reaches the call.  Values outside 0..count are
+ * left unchanged.  The context's slab scratch is shared by its calls: order calls that overlap. */
+int be_slab_relabel(be_ctx *ctx, int32_t *labels, int64_t n_rows, int32_t cols, int64_t pitch, int64_t count,
+                    int64_t offset, const int32_t *joined_labels, const int32_t *joined_targets, int32_t n_joined,
+                    void *stream);
+
 /* Report of the bounds-checked debug build (-DBE_BOUNDS_CHECK; no counterpart in the
  * reference): out3 = {site, value low, value high} of the first failed index check of the last
  * 2D (dims = 2) or 3D (dims = 3) union-find call, all zero when none failed.  Normal builds

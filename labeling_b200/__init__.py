@@ -120,6 +120,8 @@ def lib() -> ctypes.CDLL:
     l.be_stack_slices.argtypes = [vp, vp, c_int, i32, i32, i32, vp, vp]
     l.be_labels_to_rgb.argtypes = [vp, vp, i64, ctypes.c_uint32, vp, vp]
     l.be_volume_to_rgb_planes.argtypes = [vp, vp, i32, i32, i32, ctypes.c_uint32, vp, vp]
+    l.be_slab_merge.argtypes = [i32, i32, i32, vp, vp, vp, vp, p64, vp, vp, vp, i64]
+    l.be_slab_relabel.argtypes = [vp, vp, i64, i32, i64, i64, i64, vp, vp, i32, vp]
     _lib = l
     return l
 
@@ -270,6 +272,70 @@ def volume_to_rgb_planes(ctx: Context, labels, out, seed: int = 0, stream=None) 
     assert labels.is_contiguous() and out.is_contiguous() and tuple(out.shape) == (d2, d0, d1, 3)
     ctx.check(lib().be_volume_to_rgb_planes(ctx.handle, _ptr(labels), d0, d1, d2, seed & 0xFFFFFFFF,
                                             _ptr(out), _stream(stream)))
+
+
+# ---- slab split of one image (one exchange of border rows; see labeling_b200.slabs) --------
+
+class SlabMerge:
+    """Result of :func:`slab_merge`: ``offsets[s]``, ``total`` and, per slab, the ascending local
+    labels joined under an earlier piece (``joined_labels[s]``) with their final labels
+    (``joined_targets[s]``)."""
+
+    def __init__(self, offsets, total, joined_labels, joined_targets):
+        self.offsets = offsets
+        self.total = total
+        self.joined_labels = joined_labels
+        self.joined_targets = joined_targets
+
+    def lut(self, s: int, count: int) -> np.ndarray:
+        """Slab s's label map as a dense array (index = local label), for checks on the host."""
+        m = np.zeros(count + 1, np.int64)
+        loc = np.arange(1, count + 1)
+        jl = self.joined_labels[s]
+        m[1:] = self.offsets[s] + loc - np.searchsorted(jl, loc, side="left")
+        m[jl] = self.joined_targets[s]
+        return m
+
+
+def slab_merge(counts, tops: np.ndarray, bottoms: np.ndarray) -> SlabMerge:
+    """Joins slabs labeled on their own (``be_slab_merge``; host only, no GPU).  ``counts``: the
+    slabs' component counts; ``tops`` / ``bottoms``: int32 [n_slabs, cols] (2D) or
+    [n_slabs, d1, d2] (3D), each slab's first and last row (plane) of local labels."""
+    counts = np.ascontiguousarray(counts, np.int64)
+    tops = np.ascontiguousarray(tops, np.int32)
+    bottoms = np.ascontiguousarray(bottoms, np.int32)
+    n = int(counts.shape[0])
+    assert tops.shape == bottoms.shape and tops.shape[0] == n and tops.ndim in (2, 3)
+    prow, pcol = (1, int(tops.shape[1])) if tops.ndim == 2 else (int(tops.shape[1]), int(tops.shape[2]))
+    cap = 2 * prow * pcol * n
+    offsets = np.zeros(n, np.int64)
+    total = ctypes.c_int64(0)
+    jl = np.zeros(max(cap, 1), np.int32)
+    jt = np.zeros(max(cap, 1), np.int32)
+    start = np.zeros(n + 1, np.int64)
+    rc = lib().be_slab_merge(n, prow, pcol, counts.ctypes.data, tops.ctypes.data, bottoms.ctypes.data,
+                             offsets.ctypes.data, ctypes.byref(total), jl.ctypes.data, jt.ctypes.data,
+                             start.ctypes.data, cap)
+    if rc != BE_OK:
+        raise BEError(rc, "be_slab_merge: bad slab borders or counts")
+    return SlabMerge(offsets, int(total.value), [jl[start[s]:start[s + 1]].copy() for s in range(n)],
+                     [jt[start[s]:start[s + 1]].copy() for s in range(n)])
+
+
+def slab_relabel(ctx: Context, labels, count: int, offset: int, joined_labels: np.ndarray,
+                 joined_targets: np.ndarray, stream=None) -> None:
+    """Maps one slab's local labels (int32 CUDA tensor, 2D [rows, cols] or contiguous 3D
+    [planes, d1, d2]) to the whole image's labels in place (``be_slab_relabel``)."""
+    jl = np.ascontiguousarray(joined_labels, np.int32)
+    jt = np.ascontiguousarray(joined_targets, np.int32)
+    if labels.dim() == 3:
+        assert labels.is_contiguous()
+        rows, cols, pitch = int(labels.shape[0]) * int(labels.shape[1]), int(labels.shape[2]), int(labels.shape[2])
+    else:
+        rows, cols, pitch = int(labels.shape[0]), int(labels.shape[1]), int(labels.stride(0))
+    ctx.check(lib().be_slab_relabel(ctx.handle, _ptr(labels), rows, cols, pitch, int(count), int(offset),
+                                    jl.ctypes.data if jl.size else None, jt.ctypes.data if jt.size else None,
+                                    int(jl.size), _stream(stream)))
 
 
 def label2d_host(ctx: Context, img: np.ndarray, threshold: int = 0, algo: int = ALGO_AUTO,

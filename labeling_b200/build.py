@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3",
               "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 LIB_SOURCES = ["be_uf2d.cu", "be_uf3d.cu", "be_scan.cu", "be_iter.cu", "be_api.cu",
-               "be_batch.cu", "be_server.cu", "be_tune.cu", "be_noalloc.cu", "be_io.cu"]
+               "be_batch.cu", "be_server.cu", "be_tune.cu", "be_noalloc.cu", "be_io.cu", "be_slab.cu"]
 CLI_SOURCES = ["labeling.cpp", "cli_main.cpp"]
 
 

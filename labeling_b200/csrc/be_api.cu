@@ -230,6 +230,7 @@ int be_destroy(be_ctx *c)
     c->wsiter.release();
     if (c->d_in) cudaFree(c->d_in);
     if (c->d_out) cudaFree(c->d_out);
+    if (c->slab_buf) cudaFree(c->slab_buf);
     if (c->h_ncomp) cudaFreeHost(c->h_ncomp);
     for (int i = 0; i <= kStages; ++i)
         if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);

@@ -93,6 +93,8 @@ struct be_ctx {
     uint32_t *iter_err = nullptr;   // pinned: iteration-cap flag of the last iterative call
     void *d_in = nullptr, *d_out = nullptr;   // device staging of the *_host calls
     size_t d_in_bytes = 0, d_out_bytes = 0;
+    void *slab_buf = nullptr;       // be_slab_relabel: label map + joined lists
+    size_t slab_bytes = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int64_t *h_ncomp = nullptr;     // pinned

@@ -1,0 +1,93 @@
+"""Slab split of one image: each slab labeled on its own, then one exchange step.
+
+A 2D image is cut into bands of rows, a volume into bands of planes along d0 (its slowest
+dimension).  Each slab is labeled by ``be_label2d`` / ``be_label3d`` on its own GPU (one process
+per GPU, one slab per rank) or, on one GPU, one after another.  The exchange step moves only each
+slab's first and last row (plane) of labels and its component count: every rank gathers them
+(``all_gather`` over the process group -- NCCL for CUDA tensors, gloo on CPU), runs the same host
+merge (``be_slab_merge``) and maps its own slab's labels in place (``be_slab_relabel``).  The
+result equals labeling the whole image at once, canonical numbering included.
+
+The reference labels one image on one device (Labeling2015/src/LabelingAlgs.cpp:989-1084); this
+split is for images larger than one GPU's memory.  It has one collective, on the border rows only.
+"""
+from __future__ import annotations
+
+from typing import List, Tuple
+
+import numpy as np
+
+from . import Context, SlabMerge, label2d, label3d, slab_merge, slab_relabel
+
+
+def slab_bounds(n: int, parts: int) -> List[Tuple[int, int]]:
+    """``parts`` bands of ``n`` rows (planes), sizes differing by at most one, in order."""
+    if parts < 1 or parts > n:
+        raise ValueError(f"cannot cut {n} rows into {parts} non-empty slabs")
+    q, r = divmod(n, parts)
+    out, a = [], 0
+    for k in range(parts):
+        b = a + q + (1 if k < r else 0)
+        out.append((a, b))
+        a = b
+    return out
+
+
+def _borders(labels) -> Tuple[np.ndarray, np.ndarray]:
+    return labels[0].cpu().numpy(), labels[-1].cpu().numpy()
+
+
+def label_slabs(ctx: Context, img, out, parts: int, threshold: int = 0, stream=None) -> int:
+    """Labels a 2D image [rows, cols] or a volume [d0, d1, d2] (CUDA tensors; ``out`` int32 of the
+    same shape, contiguous rows) as ``parts`` slabs on this one GPU, one after another, and joins
+    them.  Returns the component count of the whole image."""
+    bounds = slab_bounds(int(img.shape[0]), parts)
+    counts, tops, bottoms = [], [], []
+    for a, b in bounds:
+        if img.dim() == 3:
+            counts.append(label3d(ctx, img[a:b], out[a:b], threshold=threshold, stream=stream))
+        else:
+            counts.append(label2d(ctx, img[a:b], out[a:b], threshold=threshold, stream=stream))
+        t, btm = _borders(out[a:b])
+        tops.append(t)
+        bottoms.append(btm)
+    m = slab_merge(counts, np.stack(tops), np.stack(bottoms))
+    for s, (a, b) in enumerate(bounds):
+        slab_relabel(ctx, out[a:b], counts[s], int(m.offsets[s]), m.joined_labels[s], m.joined_targets[s],
+                     stream=stream)
+    return m.total
+
+
+def exchange_and_merge(top, bottom, count: int, group=None) -> Tuple[int, SlabMerge]:
+    """The exchange step of rank k, which holds slab k of ``world_size`` slabs in rank order:
+    gathers every slab's border rows (``top`` / ``bottom``, int32 tensors on the group's device)
+    and count, and merges them on the host.  Returns (this rank's slab index, the merge)."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    dev = top.device
+    cnt = torch.tensor([int(count)], dtype=torch.int64, device=dev)
+    counts = [torch.empty_like(cnt) for _ in range(world)]
+    dist.all_gather(counts, cnt, group=group)
+    # Top and bottom rows travel together: one collective on the border rows.
+    both = torch.stack([top.contiguous(), bottom.contiguous()])
+    gathered = [torch.empty_like(both) for _ in range(world)]
+    dist.all_gather(gathered, both, group=group)
+    g = np.stack([x.cpu().numpy() for x in gathered])
+    m = slab_merge(np.array([int(c.item()) for c in counts], np.int64), g[:, 0], g[:, 1])
+    return rank, m
+
+
+def label_distributed(ctx: Context, slab, out, threshold: int = 0, group=None, stream=None) -> int:
+    """Rank k labels slab k (2D rows or 3D planes, on its own GPU), takes part in the exchange and
+    maps its labels to the whole image's.  Every rank must call it, with slabs in rank order and
+    equal border sizes.  Returns the component count of the whole image."""
+    if slab.dim() == 3:
+        count = label3d(ctx, slab, out, threshold=threshold, stream=stream)
+    else:
+        count = label2d(ctx, slab, out, threshold=threshold, stream=stream)
+    k, m = exchange_and_merge(out[0], out[-1], count, group=group)
+    slab_relabel(ctx, out, count, int(m.offsets[k]), m.joined_labels[k], m.joined_targets[k], stream=stream)
+    return m.total
