@@ -305,11 +305,10 @@ def bench_ours(args, rank, world, local_rank):
         stream.synchronize()
         counts = [label(i, want=True) for i in range(len(inputs))]
 
-        ctx.set_stage_timing(True)
+        # Timed steps: no events between the launches of a step (they would serialize the
+        # launches' overlapped starts); the per-launch split comes from a second pass below.
         ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        stage_ms = np.zeros(len(stages))
-        per_stage = {}
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
@@ -321,13 +320,23 @@ def bench_ours(args, rank, world, local_rank):
                 ev0[s].record(stream)
                 label(i)
                 ev1[s].record(stream)
-                st = ctx.stage_times()
-                stage_ms += np.array(st[:len(stages)])
-                per_stage.setdefault(inputs[i][0], []).append(st[:len(stages)])
                 px_done += npx[i]
             torch.cuda.synchronize()
-        ctx.set_stage_timing(False)
         step_ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
+
+        # Per-launch device times (CUDA events between the launches), same steps again.
+        ctx.set_stage_timing(True)
+        stage_ms = np.zeros(len(stages))
+        per_stage = {}
+        for s in range(args.steps):
+            i = s % len(inputs)
+            flush.fill_(s & 0xFF)
+            label(i)
+            st = ctx.stage_times()
+            stage_ms += np.array(st[:len(stages)])
+            per_stage.setdefault(inputs[i][0], []).append(st[:len(stages)])
+        torch.cuda.synchronize()
+        ctx.set_stage_timing(False)
     per_image = {}
     for s_, ms_ in enumerate(step_ms):
         per_image.setdefault(inputs[s_ % len(inputs)][0], []).append(ms_)

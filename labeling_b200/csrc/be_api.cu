@@ -170,18 +170,26 @@ cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persist
     };
     Work wk = w;
     if (!persistent) wk.queue = nullptr;
+    // The launches after the first overlap their start with the tail of the one before (they
+    // wait for it on the device); not when events are recorded between them.
+    const bool ov = !persistent && !ev;
+    cudaError_t e = cudaSuccess;
+    auto keep = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+    };
     mark(0);
     k_tile_local_3d<<<grid(w.n_tiles, 5), kT3LocalThreads, 0, s>>>(L, wk);
+    keep(cudaGetLastError());
     mark(1);
-    k_merge_3d<<<grid(w.n_tiles, 8), kT3MergeThreads, 0, s>>>(L, wk);
+    keep(launch_k(k_merge_3d, grid(w.n_tiles, 8), kT3MergeThreads, s, ov, L, wk));
     mark(2);
-    k_post_3d<<<grid(w.n_tiles + w.n_chunks, 12), kPostThreads, 0, s>>>(L, wk);
+    keep(launch_k(k_post_3d, grid(w.n_tiles + w.n_chunks, 12), kPostThreads, s, ov, L, wk));
     mark(3);
-    k_segscan<<<unsigned(std::max(w.n_chunks, 1)), kScanThreads, 0, s>>>(wk);
+    keep(launch_k(k_segscan, unsigned(std::max(w.n_chunks, 1)), kScanThreads, s, ov, wk));
     mark(4);
-    k_tile_write_3d<<<grid(w.n_tiles, 2), kT3Threads, 0, s>>>(L, wk);
+    keep(launch_k(k_tile_write_3d, grid(w.n_tiles, 2), kT3Threads, s, ov, L, wk));
     mark(5);
-    return cudaGetLastError();
+    return e;
 }
 
 }  // namespace be

@@ -14,6 +14,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <utility>
 
 namespace be {
 
@@ -331,6 +332,33 @@ __device__ __forceinline__ Img ImgList<Img>::get(int64_t tile) const
 
 using ImgList2D = ImgList<Img2D>;
 using ImgList3D = ImgList<Img3D>;
+
+// Programmatic dependent launch (sm_90 and later).  A launch made with programmatic stream
+// serialization may put its CTAs on the SMs while the grid before it in the stream still runs:
+// grid_dep_wait() blocks until that grid has completed and its writes are visible (for a normal
+// launch it returns at once), and grid_dep_release() lets the next grid's CTAs be scheduled once
+// every CTA of this grid has called it or exited.  The pipeline kernels wait before their first
+// global access, so the overlap only hides launch and ramp-up time, never a dependency.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Launches kernel k, with programmatic stream serialization when `overlap` is set.
+template <typename... P, typename... A>
+inline cudaError_t launch_k(void (*k)(P...), unsigned grid, unsigned block, cudaStream_t s, bool overlap,
+                            A &&...args)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = overlap ? 1u : 0u;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
 
 // Work distribution: with a queue counter every CTA pulls items until none are left (persistent
 // launch); without one, CTA b takes items b, b + grid, ...

@@ -9,6 +9,8 @@ namespace be {
 // counts and writes segpref[i] = sum of segcnt[0, i).  The last chunk also writes segpref[n_segs].
 __global__ void __launch_bounds__(kScanThreads) k_segscan(Work w)
 {
+    grid_dep_wait();
+    grid_dep_release();
     constexpr int NT = kScanThreads;
     constexpr int PER = kScanChunk / NT;   // 16 counts per thread
     __shared__ uint32_t tmp[NT / 32 + 1];

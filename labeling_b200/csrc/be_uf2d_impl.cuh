@@ -126,6 +126,7 @@ __device__ __forceinline__ void eunion(uint32_t *P, uint32_t a, uint32_t b)
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
 {
+    grid_dep_release();   // the merge launch may take free SMs during this grid's last wave
     __shared__ uint32_t P[NBLK];            // run starts: (slot << 12) | parent
     __shared__ __align__(16) uint8_t M[NBLK];
     __shared__ uint32_t WBL[NBLK / 32], WBR[NBLK / 32], WHC[NBLK / 32], WS[NBLK / 32], WCS[NBLK / 32];
@@ -497,6 +498,8 @@ constexpr int NLOC2 = MAXB + TBH + TBW + 2;    // local union-find size
 // tile's pairs are seen.
 __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
 {
+    grid_dep_wait();
+    grid_dep_release();
     __shared__ uint32_t qslot;
     __shared__ uint32_t lp[NLOC2];
     __shared__ uint32_t sid[TBH + TBW + 2];   // staged global node ids (kNone = none)
@@ -567,16 +570,20 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
             const uint32_t A = (r < nbr && tx + 1 < im.tiles_x) ? pe[t * NPERIM + 2 * TBW + TBH + r] : 0u;
             if (A) {
                 const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
+                uint32_t lastB = kNone;   // a node already paired with this one needs no second pair
 #pragma unroll
                 for (int d = -1; d <= 1; ++d) {
                     const int rr = r + d;
                     if (rr < 0 || rr >= nbr) continue;
                     const uint32_t nB = sid[rr];
-                    if (nB == kNone) continue;
+                    if (nB == kNone || nB == lastB) continue;
                     const uint32_t mB = smk[rr];
                     const bool c = d == 0 ? ((mA & 0xAu) && (mB & 0x5u))
                                           : d < 0 ? ((mA & 2u) && (mB & 4u)) : ((mA & 8u) && (mB & 1u));
-                    if (c) pair(ja, nA, uint32_t(SR + rr), nB);
+                    if (c) {
+                        pair(ja, nA, uint32_t(SR + rr), nB);
+                        lastB = nB;
+                    }
                 }
             }
         } else {
@@ -585,15 +592,19 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
             const uint32_t A = (c < nbc && ty + 1 < im.tiles_y) ? pe[t * NPERIM + TBW + c] : 0u;
             if (A) {
                 const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
+                uint32_t lastB = kNone;
 #pragma unroll
                 for (int d = -1; d <= 1; ++d) {
                     const int k = c + d + 1;   // staged bottom index
                     const uint32_t nB = sid[TBH + k];
-                    if (nB == kNone) continue;
+                    if (nB == kNone || nB == lastB) continue;
                     const uint32_t mB = smk[TBH + k];
                     const bool cn = d == 0 ? ((mA & 0xCu) && (mB & 0x3u))
                                            : d < 0 ? ((mA & 4u) && (mB & 2u)) : ((mA & 8u) && (mB & 1u));
-                    if (cn) pair(ja, nA, uint32_t(SD + k), nB);
+                    if (cn) {
+                        pair(ja, nA, uint32_t(SD + k), nB);
+                        lastB = nB;
+                    }
                 }
             }
         }
@@ -658,6 +669,7 @@ constexpr int RW = TW / 32;               // root-bitmap words per pixel row
 
 __global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
 {
+    grid_dep_wait();
     __shared__ __align__(16) uint16_t Ls[NBLK];
     __shared__ uint32_t LT[NBLK];
     __shared__ uint32_t RB[RBWORDS];
@@ -767,6 +779,8 @@ __global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kPostThreads) k_post_2d(ImgList2D L, Work w)
 {
+    grid_dep_wait();
+    grid_dep_release();
     __shared__ uint32_t tmp[kPostThreads / 32 + 1];
     __shared__ uint32_t qslot;
     const int64_t n = w.n_tiles + w.n_chunks;
@@ -803,16 +817,24 @@ inline cudaError_t launch(const ImgList2D &L, const Work &w, int sms, bool persi
     };
     Work wk = w;
     if (!persistent) wk.queue = nullptr;
+    // The launches after the first overlap their start with the tail of the one before (they
+    // wait for it on the device); not when events are recorded between them.
+    const bool ov = !persistent && !ev;
+    cudaError_t e = cudaSuccess;
+    auto keep = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+    };
     mark(0);
     k_tile_local_2d<<<grid(w.n_tiles, 6), K1_NT, 0, s>>>(L, wk);
+    keep(cudaGetLastError());
     mark(1);
-    k_merge_2d<<<grid(w.n_tiles, 8), K2_NT, 0, s>>>(L, wk);
+    keep(launch_k(k_merge_2d, grid(w.n_tiles, 8), K2_NT, s, ov, L, wk));
     mark(2);
-    k_post_2d<<<grid(w.n_tiles + w.n_chunks, 12), kPostThreads, 0, s>>>(L, wk);
+    keep(launch_k(k_post_2d, grid(w.n_tiles + w.n_chunks, 12), kPostThreads, s, ov, L, wk));
     mark(3);
-    k_segscan<<<unsigned(std::max(w.n_chunks, 1)), kScanThreads, 0, s>>>(wk);
+    keep(launch_k(k_segscan, unsigned(std::max(w.n_chunks, 1)), kScanThreads, s, ov, wk));
     mark(4);
-    k_tile_write_2d<<<grid(w.n_tiles, 6), K3_NT, 0, s>>>(L, wk);
+    keep(launch_k(k_tile_write_2d, grid(w.n_tiles, 6), K3_NT, s, ov, L, wk));
     mark(5);
-    return cudaGetLastError();
+    return e;
 }

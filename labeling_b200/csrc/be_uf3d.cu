@@ -237,6 +237,7 @@ __device__ __forceinline__ void split16b(uint4 v, uint32_t K, bool hi, uint32_t 
 
 __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
 {
+    grid_dep_release();   // the merge launch may take free SMs during this grid's last wave
     __shared__ uint32_t P[NBLK];               // run starts: (slot << 12) | parent
     __shared__ __align__(16) uint8_t M[NBLK];  // block masks
     __shared__ uint32_t CW[8][NT1];            // class words of every row
@@ -658,6 +659,8 @@ __device__ __forceinline__ bool staged_pos(int e, int &iu, int &iv)
 
 __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Work w)
 {
+    grid_dep_wait();
+    grid_dep_release();
     __shared__ uint32_t qslot;
     __shared__ uint32_t lp[MAXB + NPF];   // local union-find: this tile's nodes, then staged positions
     __shared__ uint32_t nbid[NPF];        // global node id across the face, kNone = none
@@ -749,11 +752,26 @@ __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Wo
             }
             if (threadIdx.x == 0) npl = 0;
             __syncthreads();
-            uint32_t pos = warp_reserve(&npl, __popc(hit));
-            while (hit) {
-                const int k = __ffs(hit) - 1;
-                hit &= hit - 1;
-                const int e = ebase + (u + 1 + k / 3 - 1) * pitch + (v + 1 + k % 3 - 1);
+            // Neighbours whose staged positions already share a local parent are one local set
+            // (mostly one node's patch across the face): the first of them stands for the others.
+            uint32_t keep = 0;
+            {
+                uint32_t h = hit, last0 = kNone, last1 = kNone;
+                while (h) {
+                    const int k = __ffs(h) - 1;
+                    h &= h - 1;
+                    const uint32_t a = lp[MAXB + ebase + (u + k / 3) * pitch + (v + k % 3)];
+                    if (a == last0 || a == last1) continue;
+                    last1 = last0;
+                    last0 = a;
+                    keep |= 1u << k;
+                }
+            }
+            uint32_t pos = warp_reserve(&npl, __popc(keep));
+            while (keep) {
+                const int k = __ffs(keep) - 1;
+                keep &= keep - 1;
+                const int e = ebase + (u + k / 3) * pitch + (v + k % 3);
                 pl[pos++] = (ja << 16) | uint32_t(e);
             }
             __syncthreads();
@@ -832,6 +850,8 @@ __device__ void post_tile_3d(const ImgList3D &L, Work &w, int64_t t)
 
 __global__ void __launch_bounds__(kPostThreads) k_post_3d(ImgList3D L, Work w)
 {
+    grid_dep_wait();
+    grid_dep_release();
     __shared__ uint32_t tmp[kPostThreads / 32 + 1];
     __shared__ uint32_t qslot;
     const int64_t n = w.n_tiles + w.n_chunks;
@@ -847,6 +867,7 @@ __global__ void __launch_bounds__(kPostThreads) k_post_3d(ImgList3D L, Work w)
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
 {
+    grid_dep_wait();
     __shared__ __align__(16) uint32_t Ls[NBLK];
     __shared__ uint32_t LT[NBLK];
     __shared__ uint32_t RB[TX * TY * RBW];
