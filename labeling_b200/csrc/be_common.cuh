@@ -229,6 +229,56 @@ __device__ __forceinline__ uint32_t gfind(uint32_t *gp, uint32_t a)
     return a;
 }
 
+// Union of two nodes by key: the root with the larger key is linked under the other, so parent
+// keys strictly decrease along every path and no link can close a cycle, whatever other threads
+// link meanwhile.  Latency, not work, is the cost (each step is an L2 round trip), so both finds
+// walk in lockstep (one round trip per step for both paths), and the first round trip also
+// fetches both keys, which are final when the two nodes are still roots.  on_link(key) is called
+// with the key of the root that was linked.
+template <typename OnLink>
+__device__ __forceinline__ void gunion_keyed(uint32_t *gp, const uint32_t *nkey, uint32_t a, uint32_t b,
+                                             OnLink on_link)
+{
+    volatile uint32_t *vp = gp;
+    uint32_t pa = vp[a], pb = vp[b];
+    uint32_t ka = __ldg(nkey + a), kb = __ldg(nkey + b);
+    for (;;) {
+        bool moved_a = false, moved_b = false;
+        while (pa != a || pb != b) {
+            const uint32_t ga = pa != a ? vp[pa] : pa;
+            const uint32_t gb = pb != b ? vp[pb] : pb;
+            if (pa != a) {
+                if (ga != pa) vp[a] = ga;   // path halving: only ever an ancestor
+                a = pa;
+                pa = ga;
+                moved_a = true;
+            }
+            if (pb != b) {
+                if (gb != pb) vp[b] = gb;
+                b = pb;
+                pb = gb;
+                moved_b = true;
+            }
+        }
+        if (a == b) return;
+        if (moved_a) ka = __ldg(nkey + a);
+        if (moved_b) kb = __ldg(nkey + b);
+        if (ka < kb) {
+            uint32_t t = a; a = b; b = t;
+            t = ka; ka = kb; kb = t;
+        }
+        const uint32_t old = atomicCAS(gp + a, a, b);
+        if (old == a) {
+            on_link(ka);
+            return;
+        }
+        // a was linked meanwhile: go on from its new parent, and re-read b too (linking under a
+        // stale b would stay correct but deepen the trees that every later find walks).
+        pa = old;
+        pb = vp[b];
+    }
+}
+
 // Read-only find (after all merges of the launch are complete).
 __device__ __forceinline__ uint32_t gfind_ro(const uint32_t *gp, uint32_t a)
 {

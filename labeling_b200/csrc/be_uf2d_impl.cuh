@@ -462,23 +462,11 @@ __device__ __forceinline__ void link_dec(const Img2D &im, Work &w, uint32_t key)
     dec_u8(w.segcnt, im.seg_base + y * im.tiles_x + x / TW);
 }
 
-// Union of two nodes of one image; the root with the larger key is linked under the other.
+// Union of two nodes of one image; the root with the larger key is linked under the other, and
+// the linked root leaves its segment's root count.
 __device__ void gunion2d(const Img2D &im, Work &w, uint32_t a, uint32_t b)
 {
-    for (;;) {
-        a = gfind(w.gp, a);
-        b = gfind(w.gp, b);
-        if (a == b) return;
-        uint32_t ka = w.nkey[a], kb = w.nkey[b];
-        if (ka < kb) {
-            uint32_t t = a; a = b; b = t;
-            t = ka; ka = kb; kb = t;
-        }
-        if (atomicCAS(&w.gp[a], a, b) == a) {
-            link_dec(im, w, ka);
-            return;
-        }
-    }
+    gunion_keyed(w.gp, w.nkey, a, b, [&](uint32_t key) { link_dec(im, w, key); });
 }
 
 }  // namespace
@@ -515,6 +503,13 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
         const int nbc = (min(TW, im.cols - tx * TW) + 1) >> 1;
         const int p = threadIdx.x;
         const uint16_t *pe = w.perim;
+        // This position's own border entry, loaded with the staging loads (the pairs use it).
+        uint32_t A = 0;
+        if (p < TBH) {
+            if (p < nbr && tx + 1 < im.tiles_x) A = pe[t * NPERIM + 2 * TBW + TBH + p];
+        } else if (p - TBH < nbc && ty + 1 < im.tiles_y) {
+            A = pe[t * NPERIM + TBW + (p - TBH)];
+        }
         for (int i = p; i < NLOC2; i += K2_NT) lp[i] = uint32_t(i);
         if (p == 0) nq = 0;
         // Stage: thread p < TBH takes right-column row p; the others take bottom-row column
@@ -567,7 +562,6 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
         if (p < TBH) {
             // Right border: neighbours in the tile to the right, same tile row.
             const int r = p;
-            const uint32_t A = (r < nbr && tx + 1 < im.tiles_x) ? pe[t * NPERIM + 2 * TBW + TBH + r] : 0u;
             if (A) {
                 const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
                 uint32_t lastB = kNone;   // a node already paired with this one needs no second pair
@@ -589,7 +583,6 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
         } else {
             // Bottom border: neighbours in the tile row below (including the diagonal tiles).
             const int c = p - TBH;
-            const uint32_t A = (c < nbc && ty + 1 < im.tiles_y) ? pe[t * NPERIM + TBW + c] : 0u;
             if (A) {
                 const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
                 uint32_t lastB = kNone;

@@ -549,21 +549,10 @@ namespace {
 
 __device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
 {
-    for (;;) {
-        a = gfind(w.gp, a);
-        b = gfind(w.gp, b);
-        if (a == b) return;
-        uint32_t ka = w.nkey[a], kb = w.nkey[b];
-        if (ka < kb) {
-            uint32_t t = a; a = b; b = t;
-            t = ka; ka = kb; kb = t;
-        }
-        if (atomicCAS(&w.gp[a], a, b) == a) {
-            const int64_t row = ka / uint32_t(im.d2), z = ka - row * im.d2;
-            dec_u8(w.segcnt, im.seg_base + row * im.t2 + z / TZ);
-            return;
-        }
-    }
+    gunion_keyed(w.gp, w.nkey, a, b, [&](uint32_t key) {
+        const int64_t row = key / uint32_t(im.d2), z = key - row * im.d2;
+        dec_u8(w.segcnt, im.seg_base + row * im.t2 + z / TZ);
+    });
 }
 
 }  // namespace
@@ -644,6 +633,15 @@ __device__ __forceinline__ uint32_t plus_entry(const Img3D &im, const TileGeo &g
     return w.perim[t * NPERIM + face_base(2 * AX + 1) + q];
 }
 
+// Tangent coordinates of position q of this tile's + face along AX.
+template <int AX>
+__device__ __forceinline__ void plus_uv(int q, int &u, int &v)
+{
+    using F = FaceAx<AX>;
+    u = q / F::TBb;
+    v = q % F::TBb;
+}
+
 // Staged position e of the face along AX -> (iu, iv) in the staged grid, or false when e lies in
 // another face's range.
 template <int AX>
@@ -669,6 +667,7 @@ __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Wo
     __shared__ uint32_t nq;
     __shared__ uint32_t pl[kT3MergeThreads * 9];   // one round's listed pairs: (node << 16) | staged
     __shared__ uint32_t npl;
+    __shared__ uint16_t own[NPLUS];       // this tile's + face entries (staged with the others)
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
         const Img3D im = L.get(t);
@@ -678,6 +677,12 @@ __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Wo
         for (int e = threadIdx.x; e < PF0; e += kT3MergeThreads) stage_face<0>(im, g, w, e, nbid, nbf);
         for (int e = threadIdx.x; e < PF1; e += kT3MergeThreads) stage_face<1>(im, g, w, e, nbid, nbf);
         for (int e = threadIdx.x; e < PF2; e += kT3MergeThreads) stage_face<2>(im, g, w, e, nbid, nbf);
+        for (int q = threadIdx.x; q < NPLUS; q += kT3MergeThreads) {
+            int u, v;
+            if (q < FaceAx<0>::NPOS) own[q] = uint16_t(plus_entry<0>(im, g, w, t, q, u, v));
+            else if (q < FaceAx<0>::NPOS + FaceAx<1>::NPOS) own[q] = uint16_t(plus_entry<1>(im, g, w, t, q - FaceAx<1>::PBASE, u, v));
+            else own[q] = uint16_t(plus_entry<2>(im, g, w, t, q - FaceAx<2>::PBASE, u, v));
+        }
         __syncthreads();
         // Staged positions of the same node that touch on the face are one element from here on
         // (a component crosses a face as a patch, not as scattered blocks): runs along each staged
@@ -726,15 +731,16 @@ __global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Wo
             int u = 0, v = 0, ebase = 0, pitch = 1;
             uint32_t A = 0;
             if (p < FaceAx<0>::NPOS) {
-                A = plus_entry<0>(im, g, w, t, p, u, v);
+                plus_uv<0>(p, u, v);
                 ebase = FaceAx<0>::EBASE; pitch = FaceAx<0>::PITCH;
             } else if (p < FaceAx<0>::NPOS + FaceAx<1>::NPOS) {
-                A = plus_entry<1>(im, g, w, t, p - FaceAx<1>::PBASE, u, v);
+                plus_uv<1>(p - FaceAx<1>::PBASE, u, v);
                 ebase = FaceAx<1>::EBASE; pitch = FaceAx<1>::PITCH;
             } else if (p < NPLUS) {
-                A = plus_entry<2>(im, g, w, t, p - FaceAx<2>::PBASE, u, v);
+                plus_uv<2>(p - FaceAx<2>::PBASE, u, v);
                 ebase = FaceAx<2>::EBASE; pitch = FaceAx<2>::PITCH;
             }
+            if (p < NPLUS) A = own[p];
             if (A && !GUARD(w, (A >> 4) < w.nb[t] && (A >> 4) < uint32_t(MAXB), 204, (uint64_t(t) << 16) | (A >> 4)))
                 A = 0;
             const uint32_t fa = A & 15u, ja = A >> 4;
