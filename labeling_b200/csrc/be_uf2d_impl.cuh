@@ -96,13 +96,28 @@ __device__ __forceinline__ uint32_t efind_ro(const uint32_t *P, uint32_t x)
     return x;
 }
 
+// As efind, also returning the root's own entry as read (the union compares the two).
+__device__ __forceinline__ uint32_t efind_e(uint32_t *P, uint32_t x, uint32_t &ev)
+{
+    uint32_t v = P[x];
+    while ((v & 0xFFFu) != x) {
+        const uint32_t y = v & 0xFFFu;
+        const uint32_t vg = P[y];
+        if ((vg & 0xFFFu) != y) P[x] = vg;
+        x = y;
+        v = vg;
+    }
+    ev = v;
+    return x;
+}
+
 __device__ __forceinline__ void eunion(uint32_t *P, uint32_t a, uint32_t b)
 {
     for (;;) {
-        a = efind(P, a);
-        b = efind(P, b);
+        uint32_t ea, eb;
+        a = efind_e(P, a, ea);
+        b = efind_e(P, b, eb);
         if (a == b) return;
-        const uint32_t ea = P[a], eb = P[b];
         if (ea < eb) {
             const uint32_t old = atomicMin(&P[b], ea);
             if ((old & 0xFFFu) == b) return;
@@ -329,7 +344,10 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
         __syncthreads();
         {
             const uint32_t nq = min(mqn, uint32_t(MQCAP));
-            for (uint32_t i = tid; i < nq; i += K1_NT) eunion(P, start_of(MQ[i] >> 16), start_of(MQ[i] & 0xFFFFu));
+            // Each thread takes a contiguous run of the queue: neighbouring links, mostly of the same
+            // rows, are merged one after another by one thread instead of racing on the same roots.
+            const uint32_t per = (nq + K1_NT - 1) / K1_NT, lo = min(nq, uint32_t(tid) * per), hi = min(nq, lo + per);
+            for (uint32_t i = lo; i < hi; ++i) eunion(P, start_of(MQ[i] >> 16), start_of(MQ[i] & 0xFFFFu));
         }
         __syncthreads();
 

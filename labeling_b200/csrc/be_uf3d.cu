@@ -194,13 +194,28 @@ __device__ __forceinline__ uint32_t efind3_ro(const uint32_t *P, uint32_t x)
     return x;
 }
 
+// As efind3, also returning the root's own entry as read (the union compares the two).
+__device__ __forceinline__ uint32_t efind3_e(uint32_t *P, uint32_t x, uint32_t &ev)
+{
+    uint32_t v = P[x];
+    while ((v & 0xFFFu) != x) {
+        const uint32_t y = v & 0xFFFu;
+        const uint32_t vg = P[y];
+        if ((vg & 0xFFFu) != y) P[x] = vg;
+        x = y;
+        v = vg;
+    }
+    ev = v;
+    return x;
+}
+
 __device__ __forceinline__ void eunion3(uint32_t *P, uint32_t a, uint32_t b)
 {
     for (;;) {
-        a = efind3(P, a);
-        b = efind3(P, b);
+        uint32_t ea, eb;
+        a = efind3_e(P, a, ea);
+        b = efind3_e(P, b, eb);
         if (a == b) return;
-        const uint32_t ea = P[a], eb = P[b];
         if (ea < eb) {
             const uint32_t old = atomicMin(&P[b], ea);
             if ((old & 0xFFFu) == b) return;
@@ -407,7 +422,9 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
             }
             __syncthreads();
             const uint32_t nq = min(mqn[nr], uint32_t(MQ1));
-            for (uint32_t q = tid; q < nq; q += NT1) eunion3(P, start_of(MQ[q] >> 16), start_of(MQ[q] & 0xFFFFu));
+            // Contiguous runs of the queue per thread, as in 2D.
+            const uint32_t per = (nq + NT1 - 1) / NT1, lo = min(nq, uint32_t(tid) * per), hi = min(nq, lo + per);
+            for (uint32_t q = lo; q < hi; ++q) eunion3(P, start_of(MQ[q] >> 16), start_of(MQ[q] & 0xFFFFu));
             __syncthreads();
         }
 
