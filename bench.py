@@ -609,6 +609,75 @@ def bench_serve(args, rank, world, local_rank):
     }
 
 
+def bench_slab(args, rank, world, local_rank):
+    """One 8192^2 image labeled as slabs joined by one exchange of border rows.  Under torchrun each
+    rank labels one slab (rows split evenly) and the ranks all_gather the border rows over NCCL; on
+    one GPU the image is cut into --parts slabs labeled in turn.  A step is one whole image; the
+    time is CUDA events around the call on each rank (host merge and border copies included), max
+    over ranks.  After timing, every rank checks its rows against the whole-image labeling."""
+    import torch
+    import labeling_b200 as be
+    from labeling_b200 import slabs
+    from labeling_b200 import workloads as W
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    fams = args.families.split(",") if args.families else list(W.FAMILIES_8192)
+    imgs = [(f, W.family_8192(f, seed=10 + i, side=8192)) for i, f in enumerate(fams)]
+    ctx = be.Context(local_rank)
+    parts = world if world > 1 else args.parts
+    lo, hi = slabs.slab_bounds(8192, world)[rank] if world > 1 else (0, 8192)
+    d_in = [torch.from_numpy(a[lo:hi]).to(dev) for _, a in imgs]
+    d_out = [torch.empty((hi - lo, 8192), dtype=torch.int32, device=dev) for _ in imgs]
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(i):
+        if world > 1:
+            return slabs.label_distributed(ctx, d_in[i], d_out[i])
+        return slabs.label_slabs(ctx, d_in[i], d_out[i], parts)
+
+    for i in range(max(args.warmup, 3)):
+        step(i % len(imgs))
+    torch.cuda.synchronize()
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    px = 0
+    if world > 1:
+        torch.distributed.barrier()
+    with ClockSampler(local_rank) as clk:
+        for s_ in range(args.steps):
+            flush.fill_(s_ & 0xFF)
+            ev0[s_].record(stream)
+            step(s_ % len(imgs))
+            ev1[s_].record(stream)
+            px += (hi - lo) * 8192
+        torch.cuda.synchronize()
+    t_ms, px_total = replicas.combine(float(sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))), float(px), device=dev)
+    # Parity: this rank's rows against the whole image labeled at once.
+    bad = 0
+    for i, (_, a) in enumerate(imgs):
+        step(i)
+        whole = torch.empty((8192, 8192), dtype=torch.int32, device=dev)
+        be.label2d(ctx, torch.from_numpy(a).to(dev), whole)
+        bad += int((whole[lo:hi] != d_out[i]).sum().item())
+    if world > 1:
+        t = torch.tensor([bad], dtype=torch.int64, device=dev)
+        torch.distributed.all_reduce(t)
+        bad = int(t.item())
+    value = px_total / (t_ms / 1e3) / 1e9
+    return {
+        "metric": "Gpx/s labeled (2D 8192^2 BE, 8-conn, slab split)", "value": round(value, 3), "unit": "Gpx/s",
+        "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": round(t_ms / args.steps, 4), "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+        "config": {"workload": "slab2d", "images": [n for n, _ in imgs], "shape": [8192, 8192],
+                   "slabs": parts, "exchange": "nccl all_gather of border rows" if world > 1 else "slabs in turn on one GPU",
+                   "l2": "flushed between steps (512 MiB write)", "parallelism": f"slabs x{parts}"},
+        "e2e": None, "mismatched_labels": bad, "clocks": clk.summary(),
+        "gpu_launches": 7 * parts * args.steps,
+    }
+
+
 def bench_reference(args, rank, world):
     """The reference's own CPU implementation of the path on the host cores, bounded samples of
     the same workload (rank 0 only)."""
@@ -643,7 +712,8 @@ def main():
     ap.add_argument("--steps", type=int, default=28)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="2d8192", choices=["2d8192", "2d2048", "3d512", "batch", "serve"])
+    ap.add_argument("--workload", default="2d8192", choices=["2d8192", "2d2048", "3d512", "batch", "serve", "slab2d"])
+    ap.add_argument("--parts", type=int, default=4, help="slab2d on one GPU: number of slabs")
     ap.add_argument("--rates", default="100,300,1000,3000,5000", help="serve: Poisson rates (req/s)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--families", default="", help="comma-separated subset of the workload's images "
@@ -667,6 +737,8 @@ def main():
         res = bench_batch(args, rank, world, local_rank)
     elif args.workload == "serve":
         res = bench_serve(args, rank, world, local_rank)
+    elif args.workload == "slab2d":
+        res = bench_slab(args, rank, world, local_rank)
     else:
         res = bench_ours(args, rank, world, local_rank)
     if world > 1:
