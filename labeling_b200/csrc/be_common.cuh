@@ -215,20 +215,6 @@ __device__ __forceinline__ uint32_t warp_reserve(uint32_t *count, uint32_t n)
     return base + incl - n;
 }
 
-// Global union-find find with path halving.  Only non-root entries are rewritten and only with an
-// ancestor, which stays correct while other threads link roots (roots change only by CAS).
-__device__ __forceinline__ uint32_t gfind(uint32_t *gp, uint32_t a)
-{
-    uint32_t p = ld_volatile(gp + a);
-    while (p != a) {
-        uint32_t g = ld_volatile(gp + p);
-        if (g != p) *reinterpret_cast<volatile uint32_t *>(gp + a) = g;
-        a = p;
-        p = g;
-    }
-    return a;
-}
-
 // Union of two nodes by key: the root with the larger key is linked under the other, so parent
 // keys strictly decrease along every path and no link can close a cycle, whatever other threads
 // link meanwhile.  Latency, not work, is the cost (each step is an L2 round trip), so both finds
