@@ -100,6 +100,25 @@ def test_merge_rejects_bad_borders():
         be.slab_merge([1], -t, -t)
 
 
+def test_merge_rejects_a_short_joined_capacity():
+    import ctypes
+    be = _lib_or_skip()
+    # Two one-row slabs whose single components join: slab 1's piece is joined under slab 0's.
+    tops = np.array([[1, 0], [1, 0]], np.int32)
+    counts = np.array([1, 1], np.int64)
+    offsets = np.zeros(2, np.int64)
+    start = np.zeros(3, np.int64)
+    total = ctypes.c_int64(0)
+    jl = np.zeros(4, np.int32)
+    jt = np.zeros(4, np.int32)
+    lib = be.lib()
+    args = (2, 1, 2, counts.ctypes.data, tops.ctypes.data, tops.ctypes.data, offsets.ctypes.data,
+            ctypes.byref(total), jl.ctypes.data, jt.ctypes.data, start.ctypes.data)
+    assert lib.be_slab_merge(*args, 0) == 1          # BE_ERR_INVALID: one joined piece, no room
+    assert lib.be_slab_merge(*args, 1) == 0
+    assert total.value == 1 and list(start) == [0, 0, 1] and jl[0] == 1 and jt[0] == 1
+
+
 def test_slab_bounds():
     assert _bounds(10, 3) == [(0, 4), (4, 7), (7, 10)]
     assert _bounds(5, 5) == [(0, 1), (1, 2), (2, 3), (3, 4), (4, 5)]
@@ -132,6 +151,45 @@ def _worker(rank, world, port, img, q):
     finally:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _worker3d(rank, world, port, vol, q):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        from labeling_b200.slabs import exchange_and_merge, slab_bounds
+        a, b = slab_bounds(vol.shape[0], world)[rank]
+        lab, k = O.ccl3d(vol[a:b], 0, True)
+        t = torch.from_numpy(lab)
+        idx, m = exchange_and_merge(t[0], t[-1], k)
+        q.put((rank, idx, m.total, m.lut(idx, k)[lab].astype(np.int32)))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def test_exchange_3d_over_two_gloo_ranks():
+    _lib_or_skip()
+    import torch.multiprocessing as mp
+    rng = np.random.default_rng(5)
+    vol = (rng.random((13, 17, 11)) < 0.3).astype(np.uint8) * 255
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker3d, args=(r, 2, port, vol, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ref, k = O.ccl3d(vol, 0, True)
+    assert all(r[1] == r[0] and r[2] == k for r in res)
+    np.testing.assert_array_equal(np.concatenate([r[3] for r in res]), ref)
 
 
 @pytest.mark.parametrize("world", [2, 3])
