@@ -91,6 +91,25 @@ def test_merge_3d_equals_whole_volume(parts):
         np.testing.assert_array_equal(got, ref, err_msg=f"{name} parts={parts}")
 
 
+def test_merge_random_sweep():
+    """Seeded sweep: random sizes, densities and slab counts, 2D and 3D, against the oracle."""
+    be = _lib_or_skip()
+    rng = np.random.default_rng(2024)
+    for it in range(60):
+        if it % 2 == 0:
+            shape = (int(rng.integers(1, 80)), int(rng.integers(1, 80)))
+            label = lambda x: O.ccl2d(x, 0, True)
+        else:
+            shape = tuple(int(v) for v in rng.integers(1, 14, size=3))
+            label = lambda x: O.ccl3d(x, 0, True)
+        img = (rng.random(shape) < rng.uniform(0.05, 0.95)).astype(np.uint8) * 255
+        parts = int(rng.integers(1, shape[0] + 1))
+        ref, k = label(img)
+        got, total = _join_on_host(be, img, parts, label)
+        assert total == k, (it, shape, parts)
+        np.testing.assert_array_equal(got, ref, err_msg=f"case {it} shape={shape} parts={parts}")
+
+
 def test_merge_rejects_bad_borders():
     be = _lib_or_skip()
     t = np.array([[1, 0, 3]], np.int32)   # label 3 > count 2
