@@ -33,25 +33,22 @@ def slab_bounds(n: int, parts: int) -> List[Tuple[int, int]]:
     return out
 
 
-def _borders(labels) -> Tuple[np.ndarray, np.ndarray]:
-    return labels[0].cpu().numpy(), labels[-1].cpu().numpy()
-
-
 def label_slabs(ctx: Context, img, out, parts: int, threshold: int = 0, stream=None) -> int:
     """Labels a 2D image [rows, cols] or a volume [d0, d1, d2] (CUDA tensors; ``out`` int32 of the
     same shape, contiguous rows) as ``parts`` slabs on this one GPU, one after another, and joins
     them.  Returns the component count of the whole image."""
+    import torch
+
     bounds = slab_bounds(int(img.shape[0]), parts)
-    counts, tops, bottoms = [], [], []
+    counts = []
     for a, b in bounds:
         if img.dim() == 3:
             counts.append(label3d(ctx, img[a:b], out[a:b], threshold=threshold, stream=stream))
         else:
             counts.append(label2d(ctx, img[a:b], out[a:b], threshold=threshold, stream=stream))
-        t, btm = _borders(out[a:b])
-        tops.append(t)
-        bottoms.append(btm)
-    m = slab_merge(counts, np.stack(tops), np.stack(bottoms))
+    # Every slab's first and last row in one device-to-host copy.
+    rows = torch.stack([out[i] for a, b in bounds for i in (a, b - 1)]).cpu().numpy()
+    m = slab_merge(counts, rows[0::2], rows[1::2])
     for s, (a, b) in enumerate(bounds):
         slab_relabel(ctx, out[a:b], counts[s], int(m.offsets[s]), m.joined_labels[s], m.joined_targets[s],
                      stream=stream)
