@@ -1,21 +1,26 @@
 """Benchmark of the B200 Block-Equivalence labeler; prints ONE JSON line (rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload 2d8192|2d2048|3d512|batch]
+                    [--workload 2d8192|2d2048|3d512|batch|serve|slab2d] [--subs LIST] [--algo uf|iter]
 
-Default workload (2d8192): 2D 8192x8192 uint8 images of the seven seeded families (Bernoulli
-p = 0.1 / 0.4 / 0.6 / 0.9, 2000 disks over p = 0.05 noise, serpentine, spiral), 8-connectivity,
-int32 labels.  One step labels one image (the families in turn), inputs resident in HBM.  The
-inputs (64 MiB) fit in L2, so a 512 MiB buffer is written between timed steps (L2 flush) and each
-step is timed alone with CUDA events on the labeling stream.
+Default run: the 2D 8192x8192 headline plus one sub-record per other configuration of the metric
+("sub": 3D 512^3, the 4096-image uneven batch against 4096 plain launches, and the served Poisson
+sweep with p50 / p99), each with its own roofline, end-to-end figure and clock record.
 
-`value` is Gpx/s over the timed steps (max over ranks for N > 1; every rank labels its own
+Headline (2d8192): the seven seeded 8192x8192 families (Bernoulli p = 0.1 / 0.4 / 0.6 / 0.9, 2000
+disks over p = 0.05 noise, serpentine, spiral), 8-connectivity, int32 labels.  One step labels one
+image (the families in turn), inputs resident in HBM.  The inputs (64 MiB) fit in L2, so a 512 MiB
+buffer is written between timed steps (L2 flush) and each step is timed alone with CUDA events on
+the labeling stream.
+
+`value` is Gpx/s over the timed steps (max time over ranks for N > 1; every rank labels its own
 images, weak scaling).  `e2e` is the same metric through the host-buffer C-ABI call
-(be_label2d_host: pinned host image -> device -> labels -> pinned host labels, wall clock).
-`roofline` takes the algorithmic 5 bytes per pixel (1 B read + 4 B label write) of the whole
-labeling over the device time of its launches; `roofline_kernels` splits it per launch.
-`cpu_baseline` times the reference's own CPU labeler (compiled from its sources into
-oracle/_ref) on the host cores, on a bounded sample.
+(be_label2d_host: pinned host image -> device -> labels -> pinned host labels, wall clock) and
+through the request API.  `roofline` takes the algorithmic 5 bytes per pixel (1 B read + 4 B label
+write) of the whole labeling over the device time of its launches; `roofline_kernels` splits it
+per launch.  `cpu_baseline` times the reference's own CPU labeler (compiled from its sources into
+oracle/_ref) on the host cores, on a bounded sample; the same leg checks every timed label map
+against the oracle (`mismatched_labels`, outside the timed region).
 
 --impl reference runs only that reference CPU labeler (all host threads) on the same workload
 and prints the same line with "impl": "reference".
@@ -25,6 +30,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import platform
 import subprocess
 import sys
 import threading
@@ -45,6 +51,21 @@ STAGES_3D = ["k_tile_local_3d", "k_merge_3d", "k_post_3d", "k_segscan", "k_tile_
 ALGO_BYTES = {"k_tile_local_2d": 1.0, "k_tile_write_2d": 4.0, "k_tile_local_3d": 1.0,
               "k_tile_write_3d": 4.0}
 
+# Bytes the union-find pipeline itself moves per pixel / voxel, by array (reads and writes of the
+# five launches, counted from the kernels' loads and stores; node records of border components,
+# at most a few bytes per border pixel, are left out).  2D tile 64 x 256 px, 3D tile 16 x 32 x 64.
+IMPL_BYTES = {
+    "2d": {"input read": 1.0, "labels written": 4.0,
+           "block entries written + read (uint16 per 2x2 block)": 2 * 0.5,
+           "root bitmap written + read (1 bit per pixel)": 2 * 0.125,
+           "border entries written + read twice": 3 * 640 / 16384,
+           "segment counts + prefix": (1 + 1 + 4 + 4) / 256},
+    "3d": {"input read": 1.0, "labels written": 4.0,
+           "block entries written + read (uint32 per 2x2x2 block)": 2 * 0.5,
+           "border entries written + read twice": 3 * 2 * (8 * 16 + 8 * 32 + 16 * 32) * 2 / 32768,
+           "segment counts + prefix": (1 + 1 + 4 + 4) / 64},
+}
+
 
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -54,6 +75,21 @@ def load_peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def host_info() -> dict:
+    """The host's CPU model, core count and OpenMP setting (for the CPU baseline records)."""
+    model = platform.processor() or ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count(),
+            "omp_num_threads": os.environ.get("OMP_NUM_THREADS", "unset (OpenMP default: all)")}
 
 
 class ClockSampler:
@@ -183,8 +219,29 @@ def make_3d_inputs(side: int, seed: int, only: str = ""):
     return out
 
 
+def make_batch_inputs(n: int, rank: int, dev):
+    """The uneven batch: n images, height and width log-uniform in [64, 2048] independently,
+    Bernoulli density per image U[0.2, 0.8] (generated on the device, seeded)."""
+    import torch
+    from labeling_b200 import workloads as W
+    sides = W.log_uniform_sides(n, 64, 2048, seed=1000 + rank)
+    rng = np.random.default_rng(2000 + rank)
+    dens = rng.uniform(0.2, 0.8, n)
+    g = torch.Generator(device=dev).manual_seed(3000 + rank)
+    d_in = [((torch.rand((h, w), generator=g, device=dev) < float(p)).to(torch.uint8) * 255)
+            for (h, w), p in zip(sides, dens)]
+    return sides, d_in
+
+
+def headline_config(workload: str, names, shape, world: int) -> dict:
+    """The `config` of a plain-labeling line; the reference arm prints the same dict."""
+    return {"workload": workload, "images": list(names), "shape": list(shape),
+            "connectivity": 26 if len(shape) == 3 else 8, "labels": "int32 canonical",
+            "l2": "flushed between steps (512 MiB write)", "parallelism": f"replicas x{world}"}
+
+
 # ------------------------------------------------------------------------------------------
-# Reference CPU labelers (oracle/_ref), bounded samples
+# Reference CPU labelers (oracle/_ref), bounded samples; parity of the timed label maps
 # ------------------------------------------------------------------------------------------
 
 CPU_ALGS_2D = {
@@ -223,7 +280,8 @@ def cpu_reference_2d(images, budget_s: float):
             O.ref_grana(img)
         t = time.perf_counter() - t0
         return {"value": sum(im.size for _, im in images[:n]) / t / 1e9, "unit": "Gpx/s", "cores": 1,
-                "kind": "reference", "sample": f"{n} whole images (gr-block, Grana, 1 thread), {t:.2f} s"}
+                "kind": "reference", "sample": f"{n} whole images (gr-block, Grana, 1 thread), {t:.2f} s",
+                **host_info()}
     cores = int(lib.ref_cpu_max_threads())
     res = {}
     for alg in CPU_ALGS_2D:
@@ -233,7 +291,7 @@ def cpu_reference_2d(images, budget_s: float):
     main = res["bleq"]
     return {"value": main["value"], "unit": "Gpx/s", "cores": cores, "kind": "reference",
             "sample": f"bleq CPU slot ({CPU_ALGS_2D['bleq']}), {main['sample']}, reference stopwatch",
-            "others": {k: v for k, v in res.items() if k != "bleq"}}
+            "others": {k: v for k, v in res.items() if k != "bleq"}, **host_info()}
 
 
 def cpu_reference_3d(volumes, budget_s: float):
@@ -259,33 +317,64 @@ def cpu_reference_3d(volumes, budget_s: float):
         if time.perf_counter() - t_start > budget_s or n >= len(volumes):
             break
     return {"value": px / t_total / 1e9, "unit": "Gvox/s", "cores": cores, "kind": "reference",
-            "sample": f"{n} whole volumes (reference bleq -3 kernels on the host, OpenMP), {t_total:.2f} s"}
+            "sample": f"{n} whole volumes (reference bleq -3 kernels on the host, OpenMP), {t_total:.2f} s",
+            **host_info()}
+
+
+def check_against_oracle(items, threads: int = 8) -> dict:
+    """Parity of timed label maps, part of the cpu_baseline leg (outside every timed region):
+    items are (name, image, labels as numpy, count); each is compared with the oracle's canonical
+    labels (oracle/be_oracle.c, union-find restatement) in a thread pool.  Returns the number of
+    differing labels and the names of the images that differ."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+
+    def one(it):
+        name, img, lab, n = it
+        ref, k = O.ccl2d(img) if img.ndim == 2 else O.ccl3d(img)
+        d = int(np.count_nonzero(lab != ref))
+        return name, d, int(n) != int(k)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        res = list(ex.map(one, items))
+    return {"mismatched_labels": int(sum(d for _, d, _ in res)),
+            "images_checked": len(res),
+            "count_mismatches": [nm for nm, _, c in res if c],
+            "mismatched_images": [nm for nm, d, _ in res if d],
+            "checker": "oracle (CPU union-find restatement), every timed image once",
+            "check_s": round(time.perf_counter() - t0, 2)}
 
 
 # ------------------------------------------------------------------------------------------
-# Our arm
+# Our arm: plain per-image calls (2D 8192^2 / 2048^2, 3D 512^3)
 # ------------------------------------------------------------------------------------------
 
-def bench_ours(args, rank, world, local_rank):
+def bench_plain(args, rank, world, local_rank, workload):
     import torch
     import labeling_b200 as be
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    is3d = args.workload == "3d512"
+    is3d = workload == "3d512"
+    algo = be.ALGO_ITER if args.algo == "iter" else be.ALGO_UF
+    form = "iterative scan/analyze" if args.algo == "iter" else "union-find"
     if is3d:
-        inputs = make_3d_inputs(512, seed=replicas.replica_seed(100, rank), only=args.families)
+        inputs = make_3d_inputs(512, seed=replicas.replica_seed(100, rank),
+                                only=args.families if args.workload == "3d512" else "")
         stages = STAGES_3D
         metric, unit = "Gvox/s labeled (3D 512^3 BE, 26-conn)", "Gvox/s"
     else:
-        side = 2048 if args.workload == "2d2048" else 8192
+        side = 2048 if workload == "2d2048" else 8192
         fams = ["bern0.5"] if side == 2048 else None
-        if args.families:
+        if args.families and args.workload == workload:
             fams = args.families.split(",")
         from labeling_b200 import workloads as W
         inputs = make_2d_inputs(side, fams or W.FAMILIES_8192, seed=replicas.replica_seed(10, rank))
         stages = STAGES_2D
         metric, unit = f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "Gpx/s"
+    if algo == be.ALGO_ITER:
+        metric = metric.replace("BE,", "BE iterative,")
 
     ctx = be.Context(local_rank)
     stream = torch.cuda.Stream(device=dev)
@@ -296,8 +385,8 @@ def bench_ours(args, rank, world, local_rank):
 
     def label(i, want=False):
         if is3d:
-            return be.label3d(ctx, d_in[i], d_out[i], want_count=want, stream=stream)
-        return be.label2d(ctx, d_in[i], d_out[i], want_count=want, stream=stream)
+            return be.label3d(ctx, d_in[i], d_out[i], want_count=want, stream=stream, algo=algo)
+        return be.label2d(ctx, d_in[i], d_out[i], want_count=want, stream=stream, algo=algo)
 
     with torch.cuda.stream(stream):
         for i in range(max(args.warmup, 3)):
@@ -325,18 +414,23 @@ def bench_ours(args, rank, world, local_rank):
         step_ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
 
         # Per-launch device times (CUDA events between the launches), same steps again.
-        ctx.set_stage_timing(True)
         stage_ms = np.zeros(len(stages))
         per_stage = {}
-        for s in range(args.steps):
-            i = s % len(inputs)
-            flush.fill_(s & 0xFF)
+        if algo == be.ALGO_UF:
+            ctx.set_stage_timing(True)
+            for s in range(args.steps):
+                i = s % len(inputs)
+                flush.fill_(s & 0xFF)
+                label(i)
+                st = ctx.stage_times()
+                stage_ms += np.array(st[:len(stages)])
+                per_stage.setdefault(inputs[i][0], []).append(st[:len(stages)])
+            torch.cuda.synchronize()
+            ctx.set_stage_timing(False)
+        # Every timed image labeled once more; its map is kept for the parity check.
+        for i in range(len(inputs)):
             label(i)
-            st = ctx.stage_times()
-            stage_ms += np.array(st[:len(stages)])
-            per_stage.setdefault(inputs[i][0], []).append(st[:len(stages)])
         torch.cuda.synchronize()
-        ctx.set_stage_timing(False)
     per_image = {}
     for s_, ms_ in enumerate(step_ms):
         per_image.setdefault(inputs[s_ % len(inputs)][0], []).append(ms_)
@@ -347,118 +441,123 @@ def bench_ours(args, rank, world, local_rank):
     # End to end through the host-buffer C-ABI call, pinned host memory.
     h_in = [torch.from_numpy(a).pin_memory() for _, a in inputs]
     h_out = [torch.empty(a.shape, dtype=torch.int32).pin_memory() for _, a in inputs]
+    host_call = be.label3d_host if is3d else be.label2d_host
     for i in range(min(2, len(inputs))):
-        (be.label3d_host if is3d else be.label2d_host)(ctx, h_in[i].numpy(), out=h_out[i].numpy())
+        host_call(ctx, h_in[i].numpy(), out=h_out[i].numpy(), algo=algo)
     t0 = time.perf_counter()
     e2e_px = 0
     e2e_steps = max(1, min(args.steps, 2 * len(inputs)))
     h2d = d2h = 0
     for s in range(e2e_steps):
         i = s % len(inputs)
-        (be.label3d_host if is3d else be.label2d_host)(ctx, h_in[i].numpy(), out=h_out[i].numpy())
+        host_call(ctx, h_in[i].numpy(), out=h_out[i].numpy(), algo=algo)
         e2e_px += npx[i]
         h2d += npx[i]
         d2h += 4 * npx[i] + 8
     e2e_s = time.perf_counter() - t0
     e2e_sync = e2e_px / e2e_s / 1e9
-    # The same host buffers through the request API (be_server_*: two lanes, so one image's
-    # upload overlaps the previous image's download -- PCIe carries both directions at once).
-    srv = be.Server(device=local_rank, lanes=2, max_batch=1)
-    for i in range(min(2, len(inputs))):
-        srv.wait(srv.submit(h_in[i].numpy(), h_out[i].numpy()))
-    t0 = time.perf_counter()
-    ids = [srv.submit(h_in[s % len(inputs)].numpy(), h_out[s % len(inputs)].numpy()) for s in range(e2e_steps)]
-    for i in ids:
-        srv.wait(i)
-    e2e_srv_s = time.perf_counter() - t0
-    srv.close()
-    e2e_srv = e2e_px / e2e_srv_s / 1e9
-    e2e = {"value": round(max(e2e_sync, e2e_srv), 4), "unit": unit, "h2d_bytes_per_step": int(h2d / e2e_steps),
-           "d2h_bytes_per_step": int(d2h / e2e_steps),
-           "per_call": round(e2e_sync, 4), "pipelined": round(e2e_srv, 4),
-           "how": ("pinned host image -> device -> labels -> pinned host, every step; 'per_call' = "
-                   "synchronous be_label*_host calls, 'pipelined' = be_server requests on two lanes "
-                   "(uploads overlap downloads); value = the better")}
+    e2e = {"value": round(e2e_sync, 4), "unit": unit, "h2d_bytes_per_step": int(h2d / e2e_steps),
+           "d2h_bytes_per_step": int(d2h / e2e_steps), "per_call": round(e2e_sync, 4),
+           "how": "pinned host image -> device -> labels -> pinned host, every step"}
+    if algo == be.ALGO_UF:
+        # The same host buffers through the request API (be_server_*: two lanes, so one image's
+        # upload overlaps the previous image's download -- PCIe carries both directions at once).
+        srv = be.Server(device=local_rank, lanes=2, max_batch=1)
+        for i in range(min(2, len(inputs))):
+            srv.wait(srv.submit(h_in[i].numpy(), h_out[i].numpy()))
+        t0 = time.perf_counter()
+        ids = [srv.submit(h_in[s % len(inputs)].numpy(), h_out[s % len(inputs)].numpy()) for s in range(e2e_steps)]
+        for i in ids:
+            srv.wait(i)
+        e2e_srv_s = time.perf_counter() - t0
+        srv.close()
+        e2e_srv = e2e_px / e2e_srv_s / 1e9
+        e2e.update({"value": round(max(e2e_sync, e2e_srv), 4), "pipelined": round(e2e_srv, 4),
+                    "how": ("pinned host image -> device -> labels -> pinned host, every step; 'per_call' = "
+                            "synchronous be_label*_host calls, 'pipelined' = be_server requests on two lanes "
+                            "(uploads overlap downloads); value = the better")})
 
     peak, peak_kind = load_peaks()
     steps = args.steps
-    pipe_ms = float(stage_ms.sum()) / steps
     px_step = px_done / steps
-    achieved = 5.0 * px_step / (pipe_ms / 1e3) / 1e9
-    kernels = []
-    for name, ms in zip(stages, stage_ms / steps):
-        ab = ALGO_BYTES.get(name, 0.0) * px_step
-        kernels.append({"kernel": name, "ms": round(float(ms), 4),
-                        "share": round(float(ms) / pipe_ms, 4) if pipe_ms else None,
-                        "algorithmic_bytes": int(ab),
-                        "achieved_gbs": round(ab / (ms / 1e3) / 1e9, 1) if ab and ms else None})
-    dom = max(kernels, key=lambda k: k["ms"])
-    # DRAM traffic of one labeling from a committed ncu capture of the same workload's image size
-    # (profiles/traffic.json): the five launches' dram__bytes_read.sum + dram__bytes_write.sum.
-    traffic, traffic_note = None, None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        try:
-            tr = json.load(open(tp)).get(args.workload)
-        except Exception:
-            tr = None
-        if tr:
-            traffic = int(tr["bytes_per_labeling"])
-            traffic_note = f"ncu, one {tr['image']} labeling, five launches"
-            for k in kernels:
-                k["traffic_bytes"] = tr["per_kernel"].get(k["kernel"])
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_note,
+    ms_step = t_ms / steps
+    impl = IMPL_BYTES["3d" if is3d else "2d"]
+    impl_bpp = float(sum(impl.values()))
+    roofline = {"bound": "hbm", "achieved": round(5.0 * px_step / (ms_step / 1e3) / 1e9, 1), "peak": peak,
+                "unit": "GB/s", "peak_kind": peak_kind,
+                "scope": "whole labeling (all launches of one call), 5 B/px over the timed ms_per_step",
                 "algorithmic_bytes_per_labeling": int(5 * px_step),
-                "peak_kind": peak_kind, "scope": "whole labeling (5 launches), 5 B/px",
-                "dominant_kernel": dom["kernel"],
-                "frac_of_8tbs": round(achieved / 8000.0, 4)}
+                "traffic": int(impl_bpp * px_step),
+                "traffic_source": ("analytic: bytes the pipeline's kernels load and store per labeling "
+                                   f"({impl_bpp:.3f} B/px = {impl_bpp / 5:.2f}x the algorithmic 5 B/px)"),
+                "traffic_by_array_bytes_per_px": {k: round(v, 4) for k, v in impl.items()}}
+    roofline["frac"] = round(roofline["achieved"] / peak, 4)
+    roofline["frac_of_8tbs"] = round(roofline["achieved"] / 8000.0, 4)
+    kernels = []
+    if algo == be.ALGO_UF:
+        pipe_ms = float(stage_ms.sum()) / steps
+        for name, ms in zip(stages, stage_ms / steps):
+            ab = ALGO_BYTES.get(name, 0.0) * px_step
+            kernels.append({"kernel": name, "ms": round(float(ms), 4),
+                            "share": round(float(ms) / pipe_ms, 4) if pipe_ms else None,
+                            "algorithmic_bytes": int(ab),
+                            "achieved_gbs": round(ab / (ms / 1e3) / 1e9, 1) if ab and ms else None})
+        roofline["dominant_kernel"] = max(kernels, key=lambda k: k["ms"])["kernel"]
+        roofline["stage_sum_ms"] = round(pipe_ms, 4)
+        # DRAM traffic of the launches from a committed ncu capture (profiles/traffic.json): a
+        # lower bound, since lines still dirty in L2 when a launch ends are written back later.
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        tr = None
+        if os.path.exists(tp):
+            try:
+                tr = json.load(open(tp)).get("3d512" if is3d else "2d8192")
+            except Exception:
+                tr = None
+        if tr:
+            roofline["traffic_ncu_lower_bound"] = int(tr["bytes_per_labeling"])
+            for k in kernels:
+                k["ncu_dram_bytes"] = tr["per_kernel"].get(k["kernel"])
     clocks = clk.summary()
 
     result = {
         "metric": metric, "value": round(value, 3), "unit": unit, "n_gpus": world,
-        "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": round(t_ms / steps, 4),
+        "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "images": [n for n, _ in inputs],
-                   "shape": list(inputs[0][1].shape), "connectivity": 26 if is3d else 8,
-                   "labels": "int32 canonical", "l2": "flushed between steps (512 MiB write)",
-                   "parallelism": f"replicas x{world}"},
+        "config": {**headline_config(workload, [n for n, _ in inputs], inputs[0][1].shape, world),
+                   "form": form},
         "e2e": e2e, "roofline": roofline, "roofline_kernels": kernels,
-        "gpu_launches": 5 * steps, "clocks": clocks,
+        "gpu_launches": (5 * steps) if algo == be.ALGO_UF else None, "clocks": clocks,
         "components": {n: c for (n, _), c in zip(inputs, counts)},
         "per_image_ms": per_image,
         "per_image_stage_ms": {k: [round(float(x), 4) for x in np.mean(v, axis=0)] for k, v in per_stage.items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         budget = 20.0
-        if is3d:
-            result["cpu_baseline"] = cpu_reference_3d(inputs, budget)
-        else:
-            result["cpu_baseline"] = cpu_reference_2d(inputs, budget)
+        result["cpu_baseline"] = (cpu_reference_3d if is3d else cpu_reference_2d)(inputs, budget)
+        items = [(n, a, o.cpu().numpy(), c) for (n, a), o, c in zip(inputs, d_out, counts)]
+        result["parity"] = check_against_oracle(items)
+        result["mismatched_labels"] = result["parity"]["mismatched_labels"]
     ctx.close()
     return result
 
 
+# ------------------------------------------------------------------------------------------
+# Batched and served forms
+# ------------------------------------------------------------------------------------------
+
 def bench_batch(args, rank, world, local_rank):
     """4096 2D images, sides log-uniform in [64, 2048], Bernoulli density U[0.2, 0.8]: one batched
     CUDA-graph launch (autotuned) against 4096 plain per-image calls, both on one stream."""
-    import ctypes
     import torch
     import labeling_b200 as be
-    from labeling_b200 import workloads as W
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     n = args.batch_images
-    sides = W.log_uniform_sides(n, 64, 2048, seed=1000 + rank)
-    rng = np.random.default_rng(2000 + rank)
-    dens = rng.uniform(0.2, 0.8, n)
-    g = torch.Generator(device=dev).manual_seed(3000 + rank)
-    d_in, d_out = [], []
-    for (h, w), p in zip(sides, dens):
-        d_in.append(((torch.rand((h, w), generator=g, device=dev) < float(p)).to(torch.uint8) * 255))
-        d_out.append(torch.empty((h, w), dtype=torch.int32, device=dev))
+    sides, d_in = make_batch_inputs(n, rank, dev)
+    d_out = [torch.empty((h, w), dtype=torch.int32, device=dev) for h, w in sides]
+    p_out = [torch.empty((h, w), dtype=torch.int32, device=dev) for h, w in sides]
     npx = sum(h * w for h, w in sides)
     ctx = be.Context(local_rank)
     stream = torch.cuda.Stream(device=dev)
@@ -484,7 +583,7 @@ def bench_batch(args, rank, world, local_rank):
         sp = stream.cuda_stream
         args_list = [(ctx.handle, x.data_ptr(), int(x.stride(0)), int(x.shape[0]), int(x.shape[1]), 0,
                       be.COH_DEFAULT, be.ALGO_UF, y.data_ptr(), int(y.stride(0)), None, sp)
-                     for x, y in zip(d_in, d_out)]
+                     for x, y in zip(d_in, p_out)]
         for a_ in args_list[:64]:
             f(*a_)
         stream.synchronize()
@@ -495,6 +594,8 @@ def bench_batch(args, rank, world, local_rank):
         p1.record(stream)
         torch.cuda.synchronize()
         plain_ms = p0.elapsed_time(p1)
+        # every batched result against its plain call (on the device, outside the timed regions)
+        differ = [i for i in range(n) if not torch.equal(d_out[i], p_out[i])]
     t_ms, px_all = replicas.combine(t_ms, float(npx * args.steps), device=dev)
     value = px_all / (t_ms / 1e3) / 1e9
     plain = npx / (plain_ms / 1e3) / 1e9
@@ -516,7 +617,7 @@ def bench_batch(args, rank, world, local_rank):
     achieved = 5.0 * npx / (t_ms / args.steps / 1e3) / 1e9
     batch.close()
     ctx.close()
-    return {
+    res = {
         "metric": "Gpx/s labeled (batched 2D BE, 4096 uneven images, one CUDA graph)",
         "value": round(value, 3), "unit": "Gpx/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": round(t_ms / args.steps, 4),
@@ -525,16 +626,27 @@ def bench_batch(args, rank, world, local_rank):
         "config": {"workload": "batch", "images": n, "side": "log-uniform [64, 2048]",
                    "density": "U[0.2, 0.8]", "pixels": npx, "l2": "inputs 1.3 GB > L2",
                    "tuned_choice": choice, "parallelism": f"replicas x{world}"},
-        "plain_per_image": {"value": round(plain, 3), "unit": "Gpx/s", "ms": round(plain_ms, 3)},
+        "plain_per_image": {"value": round(plain, 3), "unit": "Gpx/s", "ms": round(plain_ms, 3),
+                            "launches": 5 * n},
         "batched_vs_plain": round(value / world / plain, 2),
         "e2e": {"value": round(npx * e2e_steps / e2e_s / 1e9, 3), "unit": "Gpx/s",
                 "h2d_bytes_per_step": int(npx), "d2h_bytes_per_step": int(4 * npx)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                     "frac": round(achieved / peak, 4), "traffic": int(sum(IMPL_BYTES["2d"].values()) * npx),
+                     "traffic_source": "analytic (as the 2D headline, per pixel)", "peak_kind": peak_kind,
                      "scope": "whole batch (one graph), 5 B/px"},
         "gpu_launches": 5 * args.steps, "clocks": clk.summary(),
         "components_total": int(sum(counts)),
+        "batched_differs_from_plain": len(differ),
     }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        pick = np.random.default_rng(77).choice(n, min(64, n), replace=False)
+        items = [(int(i), d_in[i].cpu().numpy(), d_out[i].cpu().numpy(), counts[i]) for i in pick]
+        res["parity"] = check_against_oracle(items)
+        res["parity"]["checker"] = ("every batched image against its plain call (device compare); a seeded "
+                                    "sample of 64 against the oracle")
+        res["mismatched_labels"] = res["parity"]["mismatched_labels"]
+    return res
 
 
 def bench_serve(args, rank, world, local_rank):
@@ -572,41 +684,58 @@ def bench_serve(args, rank, world, local_rank):
     for _ in range(2):
         for i in [srv.submit(*pool[k]) for k in range(len(pool))]:
             srv.wait(i)
+    pool_counts = [None] * len(pool)
+    for k in range(len(pool)):
+        pool_counts[k] = srv.wait(srv.submit(*pool[k]))[1]
     sweep = []
-    for rate in [float(r) for r in args.rates.split(",")]:
-        srv.reset_stats()
-        n = int(min(400, max(20, rate * 2.0)))
-        gaps = rng.exponential(1.0 / rate, n)
-        picks = rng.integers(0, len(pool), n)
-        ids, px = [], 0
-        t0 = time.perf_counter()
-        t_next = t0
-        for gap, k in zip(gaps, picks):
-            t_next += gap
-            while time.perf_counter() < t_next:
-                pass
-            ids.append(srv.submit(*pool[k]))
-            px += pool[k][0].size
-        sts = [srv.wait(i)[0] for i in ids]
-        st = srv.stats()
-        sweep.append({"rate_req_s": rate, "requests": n, "ok": int(sum(1 for x in sts if x == 0)),
-                      "throughput_req_s": round(st["completed"] / max(st["wall_s"], 1e-9), 1),
-                      "throughput_gpx_s": round(st["pixels"] / max(st["wall_s"], 1e-9) / 1e9, 3),
-                      "p50_ms": round(st["p50_us"] / 1e3, 3), "p99_ms": round(st["p99_us"] / 1e3, 3),
-                      "batches": int(st["batches"])})
+    h2d = d2h = n_req = 0
+    with ClockSampler(local_rank) as clk:
+        for rate in [float(r) for r in args.rates.split(",")]:
+            srv.reset_stats()
+            n = int(min(400, max(20, rate * 2.0)))
+            gaps = rng.exponential(1.0 / rate, n)
+            picks = rng.integers(0, len(pool), n)
+            ids, px = [], 0
+            t0 = time.perf_counter()
+            t_next = t0
+            for gap, k in zip(gaps, picks):
+                t_next += gap
+                while time.perf_counter() < t_next:
+                    pass
+                ids.append(srv.submit(*pool[k]))
+                px += pool[k][0].size
+                h2d += pool[k][0].size
+                d2h += 4 * pool[k][0].size
+                n_req += 1
+            sts = [srv.wait(i)[0] for i in ids]
+            st = srv.stats()
+            sweep.append({"rate_req_s": rate, "requests": n, "ok": int(sum(1 for x in sts if x == 0)),
+                          "throughput_req_s": round(st["completed"] / max(st["wall_s"], 1e-9), 1),
+                          "throughput_gpx_s": round(st["pixels"] / max(st["wall_s"], 1e-9) / 1e9, 3),
+                          "p50_ms": round(st["p50_us"] / 1e3, 3), "p99_ms": round(st["p99_us"] / 1e3, 3),
+                          "batches": int(st["batches"])})
     srv.close()
     best = max(sweep, key=lambda r: r["throughput_gpx_s"])
-    return {
+    res = {
         "metric": "served mixed 2D/3D stream: sustained Gpx/s with p50/p99 latency (Poisson sweep)",
         "value": best["throughput_gpx_s"], "unit": "Gpx/s", "n_gpus": world, "steps": len(sweep),
-        "warmup": 4 + 2 * len(pool), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "warmup": 4 + 3 * len(pool), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
         "config": {"workload": "serve", "mix": "80% 2D side 256-8192, 20% 3D side 64-384 (GRF 60th pct)",
-                   "pool": len(pool), "lanes": 2, "max_batch": 64, "host_buffers": "pinned"},
-        "e2e": {"value": best["throughput_gpx_s"], "unit": "Gpx/s", "h2d_bytes_per_step": None,
-                "d2h_bytes_per_step": None},
-        "sweep": sweep,
+                   "pool": len(pool), "lanes": 2, "max_batch": 64, "host_buffers": "pinned",
+                   "rates_req_s": [r["rate_req_s"] for r in sweep]},
+        "e2e": {"value": best["throughput_gpx_s"], "unit": "Gpx/s",
+                "h2d_bytes_per_step": int(h2d / max(n_req, 1)), "d2h_bytes_per_step": int(d2h / max(n_req, 1)),
+                "how": "every request: pinned host image in, labels back to pinned host; a step = one request"},
+        "sweep": sweep, "clocks": clk.summary(),
+        "p50_p99_ms_by_rate": {str(int(r["rate_req_s"])): [r["p50_ms"], r["p99_ms"]] for r in sweep},
     }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        items = [(k, a, o.copy(), c) for k, ((a, o), c) in enumerate(zip(pool, pool_counts))]
+        res["parity"] = check_against_oracle(items)
+        res["parity"]["checker"] = "every pool request's served result against the oracle"
+        res["mismatched_labels"] = res["parity"]["mismatched_labels"]
+    return res
 
 
 def bench_slab(args, rank, world, local_rank):
@@ -678,50 +807,82 @@ def bench_slab(args, rank, world, local_rank):
     }
 
 
+# ------------------------------------------------------------------------------------------
+# Reference arm
+# ------------------------------------------------------------------------------------------
+
 def bench_reference(args, rank, world):
     """The reference's own CPU implementation of the path on the host cores, bounded samples of
-    the same workload (rank 0 only)."""
+    the same workload (rank 0 only), with the same `config` as our arm's line."""
     if rank != 0:
         return None
-    is3d = args.workload == "3d512"
-    if is3d:
-        inputs = make_3d_inputs(512, seed=100)
-        cb = cpu_reference_3d(inputs, budget_s=40.0)
-        metric, unit = "Gvox/s labeled (3D 512^3 BE, 26-conn)", "Gvox/s"
-        names = [n for n, _ in inputs]
-    else:
-        side = 2048 if args.workload == "2d2048" else 8192
-        from labeling_b200 import workloads as W
-        names = ["bern0.5"] if side == 2048 else W.FAMILIES_8192
-        inputs = make_2d_inputs(side, names, seed=10)
-        cb = cpu_reference_2d(inputs, budget_s=30.0)
-        metric, unit = f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "Gpx/s"
-    if cb is None:
+
+    def one(workload, budget):
+        if workload == "3d512":
+            inputs = make_3d_inputs(512, seed=100)
+            cb = cpu_reference_3d(inputs, budget_s=budget)
+            metric, unit = "Gvox/s labeled (3D 512^3 BE, 26-conn)", "Gvox/s"
+        else:
+            side = 2048 if workload == "2d2048" else 8192
+            from labeling_b200 import workloads as W
+            names = ["bern0.5"] if side == 2048 else W.FAMILIES_8192
+            if args.families and args.workload == workload:
+                names = args.families.split(",")
+            inputs = make_2d_inputs(side, names, seed=10)
+            cb = cpu_reference_2d(inputs, budget_s=budget)
+            metric, unit = f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "Gpx/s"
+        if cb is None:
+            return None
+        form = "iterative scan/analyze" if args.algo == "iter" else "union-find"
+        if args.algo == "iter":
+            metric = metric.replace("BE,", "BE iterative,")
+        return {"impl": "reference", "metric": metric, "value": round(cb["value"], 4),
+                "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic (seeded)",
+                "config": {**headline_config(workload, [n for n, _ in inputs], inputs[0][1].shape, world),
+                           "form": form},
+                "cpu_baseline": cb, "e2e": {"value": round(cb["value"], 4), "unit": unit,
+                                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+    if args.workload not in ("2d8192", "2d2048", "3d512"):
+        return {"impl": "reference", "unavailable": f"the reference has no {args.workload} form "
+                "(batching, serving and slab splits are this project's additions)"}
+    res = one(args.workload, 40.0 if args.workload == "3d512" else 30.0)
+    if res is None:
         return {"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}
-    return {"impl": "reference", "metric": metric, "value": round(cb["value"], 4),
-            "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-            "data": "synthetic (seeded)", "config": {"workload": args.workload, "images": names},
-            "cpu_baseline": cb, "e2e": {"value": round(cb["value"], 4), "unit": unit,
-                                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    subs = [s for s in args.subs.split(",") if s] if args.workload == "2d8192" else []
+    if "3d512" in subs:
+        r3 = one("3d512", 30.0)
+        if r3 is not None:
+            res["sub"] = {"3d512": r3}
+    return res
 
 
-def main():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=28)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="2d8192", choices=["2d8192", "2d2048", "3d512", "batch", "serve", "slab2d"])
+    ap.add_argument("--subs", default="3d512,batch,serve",
+                    help="with the 2d8192 headline: the other configurations measured in the same run, "
+                         "as sub-records (empty string: none)")
+    ap.add_argument("--algo", default="uf", choices=["uf", "iter"],
+                    help="plain workloads: union-find form (default) or the iterative scan/analyze form")
     ap.add_argument("--parts", type=int, default=4, help="slab2d on one GPU: number of slabs")
     ap.add_argument("--rates", default="100,300,1000,3000,5000", help="serve: Poisson rates (req/s)")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg (and its parity check)")
     ap.add_argument("--families", default="", help="comma-separated subset of the workload's images "
                     "(2D families, or 3D bern0.1,bern0.3,bern0.5,grf50,grf80), for profiling captures")
     ap.add_argument("--batch-images", type=int, default=4096)
     ap.add_argument("--pool", type=int, default=40, help="serve: pre-generated requests")
-    args = ap.parse_args()
+    return ap.parse_args(argv)
 
+
+def main():
+    args = parse_args()
     rank, world, local_rank = replicas.rank_info()
     if args.impl == "reference":
         res = bench_reference(args, rank, world)
@@ -740,7 +901,26 @@ def main():
     elif args.workload == "slab2d":
         res = bench_slab(args, rank, world, local_rank)
     else:
-        res = bench_ours(args, rank, world, local_rank)
+        res = bench_plain(args, rank, world, local_rank, args.workload)
+        subs = [s for s in args.subs.split(",") if s] if args.workload == "2d8192" else []
+        if subs:
+            import torch
+            res["sub"] = {}
+            for s in subs:
+                torch.cuda.empty_cache()
+                if s == "3d512":
+                    r = bench_plain(args, rank, world, local_rank, "3d512")
+                elif s == "batch":
+                    r = bench_batch(args, rank, world, local_rank)
+                elif s == "serve":
+                    r = bench_serve(args, rank, world, local_rank)
+                else:
+                    raise SystemExit(f"unknown sub-record {s}")
+                for k in ("higher_is_better", "scaling", "vs_baseline", "dtype", "data", "n_gpus"):
+                    r.pop(k, None)
+                res["sub"][s] = r
+            launches = [res.get("gpu_launches") or 0] + [r.get("gpu_launches") or 0 for r in res["sub"].values()]
+            res["gpu_launches_all_records"] = int(sum(launches))
     if world > 1:
         import torch
         torch.distributed.barrier()

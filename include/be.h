@@ -206,10 +206,15 @@ int be_label2d_noalloc(const uint8_t *in, int64_t in_pitch, int32_t rows, int32_
 
 /* ---- Ingest and egress on the device (the steps either side of the labeling path) ---------------
  * be_to_gray replaces ILabeling::RGB2Gray (Labeling2015/src/LabelingTools.cpp:39-49): channels 1
- * (gray) or 3 (RGB order, cv::COLOR_RGB2GRAY: Y = (4899 R + 9617 G + 1868 B + 2^13) >> 14), then
- * with binarize != 0 the reference's fixed threshold, Y > 8 ? 255 : 0.  Pitches in bytes. */
+ * (gray) or 3 (RGB order, cv::COLOR_RGB2GRAY), then with BE_GRAY_BINARIZE the reference's fixed
+ * threshold, Y > 8 ? 255 : 0.  The gray weights are OpenCV 3.0.0's, the version the reference
+ * builds against: Y = (4899 R + 9617 G + 1868 B + 2^13) >> 14; with BE_GRAY_OPENCV4 those of
+ * OpenCV 4: Y = (9798 R + 19235 G + 3735 B + 2^14) >> 15 (within one gray level of the former).
+ * flags = 0 / 1 keeps the meaning of the former `binarize` argument.  Pitches in bytes. */
+#define BE_GRAY_BINARIZE 1
+#define BE_GRAY_OPENCV4 2
 int be_to_gray(be_ctx *ctx, const uint8_t *in, int64_t in_pitch, int channels, int32_t rows, int32_t cols,
-               int binarize, uint8_t *out, int64_t out_pitch, void *stream);
+               int flags, uint8_t *out, int64_t out_pitch, void *stream);
 
 /* be_stack_slices replaces the slice stacking of Read3DImage (Labeling2015/main.cpp:172-212):
  * `planes` slices of rows x cols pixels (channels 1 or 3, packed slice after slice) become the
@@ -257,10 +262,18 @@ int be_slab_merge(int32_t n_slabs, int32_t plane_rows, int32_t plane_cols, const
  * below l).  joined_labels (ascending) / joined_targets are HOST arrays of n_joined entries, as
  * be_slab_merge returns them for this slab; pageable memory is read before the call returns,
  * pinned memory must stay valid until the stream reaches the call.  Values outside 0..count are
- * left unchanged.  The context's slab scratch is shared by its calls: order calls that overlap. */
+ * left unchanged.  The context's slab scratch is shared by its calls: order calls that overlap.
+ * The scratch grows inside the call when count or n_joined exceed what the context holds (a
+ * device allocation, which synchronizes the device); be_slab_reserve sizes it beforehand. */
 int be_slab_relabel(be_ctx *ctx, int32_t *labels, int64_t n_rows, int32_t cols, int64_t pitch, int64_t count,
                     int64_t offset, const int32_t *joined_labels, const int32_t *joined_targets, int32_t n_joined,
                     void *stream);
+
+/* be_slab_reserve: sizes the context's slab scratch for later be_slab_relabel calls of up to
+ * max_count local labels and max_joined joined labels, so that those calls allocate nothing.
+ * A slab of n pixels has at most n / 2 + 1 components (8-connectivity), and at most
+ * 2 x (border row or plane size) joined labels. */
+int be_slab_reserve(be_ctx *ctx, int64_t max_count, int64_t max_joined);
 
 /* Report of the bounds-checked debug build (-DBE_BOUNDS_CHECK; no counterpart in the
  * reference): out3 = {site, value low, value high} of the first failed index check of the last

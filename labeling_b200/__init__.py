@@ -122,6 +122,7 @@ def lib() -> ctypes.CDLL:
     l.be_volume_to_rgb_planes.argtypes = [vp, vp, i32, i32, i32, ctypes.c_uint32, vp, vp]
     l.be_slab_merge.argtypes = [i32, i32, i32, vp, vp, vp, vp, p64, vp, vp, vp, i64]
     l.be_slab_relabel.argtypes = [vp, vp, i64, i32, i64, i64, i64, vp, vp, i32, vp]
+    l.be_slab_reserve.argtypes = [vp, i64, i64]
     _lib = l
     return l
 
@@ -238,13 +239,18 @@ def label3d(ctx: Context, vol, out, threshold: int = 0, algo: int = ALGO_AUTO,
 
 # ---- ingest and egress on the device (RGB2Gray, Read3DImage, LabelsToRGB, Write3DLabels) -----
 
-def to_gray(ctx: Context, img, out, binarize: bool = True, stream=None) -> None:
+GRAY_BINARIZE, GRAY_OPENCV4 = 1, 2
+
+
+def to_gray(ctx: Context, img, out, binarize: bool = True, opencv4: bool = False, stream=None) -> None:
     """uint8 CUDA tensor [rows, cols] or [rows, cols, 3] (RGB) -> uint8 [rows, cols]: gray as
-    cv::COLOR_RGB2GRAY, then (binarize) the reference's fixed threshold, gray > 8 ? 255 : 0."""
+    cv::COLOR_RGB2GRAY, then (binarize) the reference's fixed threshold, gray > 8 ? 255 : 0.
+    The gray weights are OpenCV 3.0.0's (the reference's OpenCV), or OpenCV 4's with opencv4."""
     channels = int(img.shape[2]) if img.dim() == 3 else 1
     rows, cols = int(img.shape[0]), int(img.shape[1])
+    flags = (GRAY_BINARIZE if binarize else 0) | (GRAY_OPENCV4 if opencv4 else 0)
     ctx.check(lib().be_to_gray(ctx.handle, _ptr(img), int(img.stride(0)), channels, rows, cols,
-                               int(bool(binarize)), _ptr(out), int(out.stride(0)), _stream(stream)))
+                               flags, _ptr(out), int(out.stride(0)), _stream(stream)))
 
 
 def stack_slices(ctx: Context, slices, out, stream=None) -> None:
@@ -320,6 +326,13 @@ def slab_merge(counts, tops: np.ndarray, bottoms: np.ndarray) -> SlabMerge:
         raise BEError(rc, "be_slab_merge: bad slab borders or counts")
     return SlabMerge(offsets, int(total.value), [jl[start[s]:start[s + 1]].copy() for s in range(n)],
                      [jt[start[s]:start[s + 1]].copy() for s in range(n)])
+
+
+def slab_reserve(ctx: Context, max_count: int, max_joined: int) -> None:
+    """Sizes the context's slab scratch so that later :func:`slab_relabel` calls of up to
+    ``max_count`` local labels and ``max_joined`` joined labels allocate nothing
+    (``be_slab_reserve``)."""
+    ctx.check(lib().be_slab_reserve(ctx.handle, int(max_count), int(max_joined)))
 
 
 def slab_relabel(ctx: Context, labels, count: int, offset: int, joined_labels: np.ndarray,

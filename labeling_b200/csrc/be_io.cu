@@ -19,26 +19,30 @@ using namespace be;
 
 namespace {
 
-// cv::cvtColor RGB -> gray for 8-bit data: Y = (R*4899 + G*9617 + B*1868 + 2^13) >> 14 (OpenCV's
-// 14-bit fixed-point form of 0.299 / 0.587 / 0.114).
-__device__ __forceinline__ uint32_t rgb_gray(uint32_t r, uint32_t g, uint32_t b)
+// cv::cvtColor RGB -> gray for 8-bit data, Y = 0.299 R + 0.587 G + 0.114 B in fixed point.  OpenCV
+// 3.0.0 (the version the reference builds against) rounds with 14-bit weights:
+// Y = (R*4899 + G*9617 + B*1868 + 2^13) >> 14; OpenCV 4 with 15-bit weights that sum to 2^15:
+// Y = (R*9798 + G*19235 + B*3735 + 2^14) >> 15 (BE_GRAY_OPENCV4).  The two differ by at most one
+// gray level on some colours.
+__device__ __forceinline__ uint32_t rgb_gray(uint32_t r, uint32_t g, uint32_t b, bool cv4)
 {
-    return (r * 4899u + g * 9617u + b * 1868u + (1u << 13)) >> 14;
+    return cv4 ? (r * 9798u + g * 19235u + b * 3735u + (1u << 14)) >> 15
+               : (r * 4899u + g * 9617u + b * 1868u + (1u << 13)) >> 14;
 }
 
-__device__ __forceinline__ uint8_t pixel_gray(const uint8_t *p, int channels, int binarize)
+__device__ __forceinline__ uint8_t pixel_gray(const uint8_t *p, int channels, int flags)
 {
-    const uint32_t y = channels == 3 ? rgb_gray(p[0], p[1], p[2]) : p[0];
-    return binarize ? (y > 8u ? 255u : 0u) : uint8_t(y);
+    const uint32_t y = channels == 3 ? rgb_gray(p[0], p[1], p[2], (flags & BE_GRAY_OPENCV4) != 0) : p[0];
+    return (flags & BE_GRAY_BINARIZE) ? (y > 8u ? 255u : 0u) : uint8_t(y);
 }
 
-__global__ void k_to_gray(const uint8_t *in, int64_t in_pitch, int channels, int rows, int cols, int binarize,
+__global__ void k_to_gray(const uint8_t *in, int64_t in_pitch, int channels, int rows, int cols, int flags,
                           uint8_t *out, int64_t out_pitch)
 {
     const int64_t n = int64_t(rows) * cols;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         const int64_t y = i / cols, x = i - y * cols;
-        out[y * out_pitch + x] = pixel_gray(in + y * in_pitch + x * channels, channels, binarize);
+        out[y * out_pitch + x] = pixel_gray(in + y * in_pitch + x * channels, channels, flags);
     }
 }
 
@@ -57,7 +61,7 @@ __global__ void __launch_bounds__(TT * 8) k_stack_slices(const uint8_t *slices, 
     for (int k = ty; k < TT; k += 8) {
         const int p = p0 + k, j = j0 + tx;
         uint8_t v = 0;
-        if (p < planes && j < cols) v = pixel_gray(slices + p * slice + (int64_t(i) * cols + j) * channels, channels, 1);
+        if (p < planes && j < cols) v = pixel_gray(slices + p * slice + (int64_t(i) * cols + j) * channels, channels, BE_GRAY_BINARIZE);
         tile[k][tx] = v;
     }
     __syncthreads();
@@ -138,16 +142,16 @@ int finish(be_ctx *c, const char *what)
 extern "C" {
 
 int be_to_gray(be_ctx *c, const uint8_t *in, int64_t in_pitch, int channels, int32_t rows, int32_t cols,
-               int binarize, uint8_t *out, int64_t out_pitch, void *stream)
+               int flags, uint8_t *out, int64_t out_pitch, void *stream)
 {
     if (!c) return BE_ERR_INVALID;
     c->err.clear();
     if (!in || !out || rows <= 0 || cols <= 0 || (channels != 1 && channels != 3) ||
-        in_pitch < int64_t(cols) * channels || out_pitch < cols)
+        in_pitch < int64_t(cols) * channels || out_pitch < cols || (flags & ~(BE_GRAY_BINARIZE | BE_GRAY_OPENCV4)))
         return set_error(c, BE_ERR_INVALID, "be_to_gray: bad arguments");
     cudaSetDevice(c->device);
     k_to_gray<<<grid_for(c, int64_t(rows) * cols), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        in, in_pitch, channels, rows, cols, binarize, out, out_pitch);
+        in, in_pitch, channels, rows, cols, flags, out, out_pitch);
     return finish(c, "be_to_gray");
 }
 

@@ -4,9 +4,11 @@
 // main.cpp:309-340; Process3DImages, :495-514).  The server instead accepts requests from any
 // thread at any time:
 //   * admission: a request is admitted when its device memory (input, labels, its share of the
-//     pipeline workspace) fits the byte budget -- by default 80% of the device's free memory at
-//     creation -- and a lane (CUDA stream) is free; otherwise it waits in the queue, and a request
-//     that could never fit is refused with BE_ERR_BUSY;
+//     pipeline workspace) fits both the byte budget -- by default 80% of the device's free memory
+//     at creation -- and the memory free on the device right now (cudaMemGetInfo plus what the
+//     server's own pool holds unused, read each time a batch is formed, so memory another tenant
+//     of the GPU took after creation is seen), and a lane (CUDA stream) is free; otherwise it waits
+//     in the queue, and a request that could never fit the budget is refused with BE_ERR_BUSY;
 //   * batching: every time a lane is free, all admitted waiting requests (up to max_batch) are
 //     copied in and labeled together by the persistent-kernel pipeline of be_batch (2D and 3D in one
 //     go), so requests that arrive while others run join the next batch;
@@ -99,6 +101,7 @@ struct be_server {
     int64_t alloc_count = 0;
 
     void run();
+    size_t live_headroom();
     bool launch(Lane &ln, std::vector<Req *> &batch);
     void finish(Lane &ln, int status);
     void *alloc(size_t bytes, cudaStream_t s, int *status);
@@ -118,6 +121,23 @@ void *be_server::alloc(size_t bytes, cudaStream_t s, int *status)
         return nullptr;
     }
     return p;
+}
+
+// Device memory a new batch can take now: free memory plus what the pool holds but does not use.
+size_t be_server::live_headroom()
+{
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    unsigned long long reserved = 0, in_use = 0;   // the pool attributes are 64-bit
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &in_use) != cudaSuccess) {
+        cudaGetLastError();
+        reserved = in_use = 0;
+    }
+    return fr + size_t(reserved > in_use ? reserved - in_use : 0);
 }
 
 // Copies in, labels and copies out one batch on lane `ln`; false when nothing could be started.
@@ -309,6 +329,8 @@ void be_server::run()
         bool started = false;
         if (free_lane && !pending.empty()) {
             std::vector<Req *> batch;
+            const size_t live = live_headroom();
+            size_t take = 0;
             while (!pending.empty() && int(batch.size()) < cfg.max_batch) {
                 Req *q = pending.front();
                 if (q->cancelled) {
@@ -328,6 +350,8 @@ void be_server::run()
                     continue;
                 }
                 if (used + need > budget) break;   // wait for memory to free up
+                if (take + need > live) break;     // the device is fuller than the budget says
+                take += need;
                 pending.pop_front();
                 q->bytes = need;
                 used += need;

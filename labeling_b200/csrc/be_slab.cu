@@ -218,7 +218,39 @@ unsigned slab_grid(const be_ctx *c, int64_t n)
 
 size_t al256(size_t v) { return (v + 255) / 256 * 256; }
 
+// Grows the context's slab scratch (label map + joined lists) to hold `need` bytes.
+int slab_scratch(be_ctx *c, size_t need)
+{
+    if (need <= c->slab_bytes) return BE_OK;
+    if (c->slab_buf) cudaFree(c->slab_buf);
+    c->slab_buf = nullptr;
+    c->slab_bytes = 0;
+    cudaError_t e = cudaMalloc(&c->slab_buf, need);
+    if (e != cudaSuccess) {
+        c->slab_buf = nullptr;
+        return cuda_error(c, e, "be_slab scratch: cudaMalloc");
+    }
+    c->slab_bytes = need;
+    return BE_OK;
+}
+
+size_t slab_bytes_for(int64_t count, int64_t n_joined)
+{
+    return al256(size_t(count + 1) * sizeof(int32_t)) + 2 * al256(size_t(n_joined) * sizeof(int32_t));
+}
+
 }  // namespace
+
+extern "C" int be_slab_reserve(be_ctx *c, int64_t max_count, int64_t max_joined)
+{
+    if (!c) return BE_ERR_INVALID;
+    c->err.clear();
+    if (max_count < 0 || max_count > INT32_MAX || max_joined < 0 || max_joined > INT32_MAX)
+        return set_error(c, BE_ERR_INVALID, "be_slab_reserve: bad sizes");
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_error(c, e, "cudaSetDevice");
+    return slab_scratch(c, slab_bytes_for(max_count, max_joined));
+}
 
 extern "C" int be_slab_relabel(be_ctx *c, int32_t *labels, int64_t n_rows, int32_t cols, int64_t pitch,
                                int64_t count, int64_t offset, const int32_t *joined_labels,
@@ -237,18 +269,8 @@ extern "C" int be_slab_relabel(be_ctx *c, int32_t *labels, int64_t n_rows, int32
     if (n_joined > 0) {
         const size_t o_jl = al256(size_t(count + 1) * sizeof(int32_t));
         const size_t o_jt = o_jl + al256(size_t(n_joined) * sizeof(int32_t));
-        const size_t need = o_jt + al256(size_t(n_joined) * sizeof(int32_t));
-        if (need > c->slab_bytes) {
-            if (c->slab_buf) cudaFree(c->slab_buf);
-            c->slab_buf = nullptr;
-            c->slab_bytes = 0;
-            e = cudaMalloc(&c->slab_buf, need);
-            if (e != cudaSuccess) {
-                c->slab_buf = nullptr;
-                return cuda_error(c, e, "be_slab_relabel: cudaMalloc");
-            }
-            c->slab_bytes = need;
-        }
+        const int rc = slab_scratch(c, slab_bytes_for(count, n_joined));
+        if (rc) return rc;
         char *base = static_cast<char *>(c->slab_buf);
         int32_t *d_map = reinterpret_cast<int32_t *>(base);
         int32_t *d_jl = reinterpret_cast<int32_t *>(base + o_jl), *d_jt = reinterpret_cast<int32_t *>(base + o_jt);

@@ -9,7 +9,9 @@ merge (``be_slab_merge``) and maps its own slab's labels in place (``be_slab_rel
 result equals labeling the whole image at once, canonical numbering included.
 
 The reference labels one image on one device (Labeling2015/src/LabelingAlgs.cpp:989-1084); this
-split is for images larger than one GPU's memory.  It has one collective, on the border rows only.
+split is for images larger than one GPU's memory.  It has one collective: an all_gather of each
+slab's border rows with its count packed in the same tensor.  The relabel scratch is sized before
+the slabs are labeled (``slab_reserve``), so the exchange and relabel allocate nothing.
 """
 from __future__ import annotations
 
@@ -17,7 +19,7 @@ from typing import List, Tuple
 
 import numpy as np
 
-from . import Context, SlabMerge, label2d, label3d, slab_merge, slab_relabel
+from . import Context, SlabMerge, label2d, label3d, slab_merge, slab_relabel, slab_reserve
 
 
 def slab_bounds(n: int, parts: int) -> List[Tuple[int, int]]:
@@ -33,6 +35,16 @@ def slab_bounds(n: int, parts: int) -> List[Tuple[int, int]]:
     return out
 
 
+def _reserve(ctx: Context, slab_shape, n_slabs: int = 1) -> None:
+    """Relabel scratch for a slab of this shape: at most one component per two pixels (plus one),
+    at most every label of both border rows (planes) of every slab joined."""
+    n = 1
+    for d in slab_shape:
+        n *= int(d)
+    plane = n // int(slab_shape[0])
+    slab_reserve(ctx, n // 2 + 1, 2 * plane * n_slabs)
+
+
 def label_slabs(ctx: Context, img, out, parts: int, threshold: int = 0, stream=None) -> int:
     """Labels a 2D image [rows, cols] or a volume [d0, d1, d2] (CUDA tensors; ``out`` int32 of the
     same shape, contiguous rows) as ``parts`` slabs on this one GPU, one after another, and joins
@@ -40,6 +52,7 @@ def label_slabs(ctx: Context, img, out, parts: int, threshold: int = 0, stream=N
     import torch
 
     bounds = slab_bounds(int(img.shape[0]), parts)
+    _reserve(ctx, (bounds[0][1] - bounds[0][0],) + tuple(img.shape[1:]), parts)
     counts = []
     for a, b in bounds:
         if img.dim() == 3:
@@ -65,15 +78,16 @@ def exchange_and_merge(top, bottom, count: int, group=None) -> Tuple[int, SlabMe
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
     dev = top.device
-    cnt = torch.tensor([int(count)], dtype=torch.int64, device=dev)
-    counts = [torch.empty_like(cnt) for _ in range(world)]
-    dist.all_gather(counts, cnt, group=group)
-    # Top and bottom rows travel together: one collective on the border rows.
-    both = torch.stack([top.contiguous(), bottom.contiguous()])
+    # Top row, bottom row and the count (a label count fits int32: images have < 2^31 pixels)
+    # travel in one tensor: one collective.
+    n = top.numel()
+    both = torch.cat([top.contiguous().reshape(-1), bottom.contiguous().reshape(-1),
+                      torch.tensor([int(count)], dtype=torch.int32, device=dev)])
     gathered = [torch.empty_like(both) for _ in range(world)]
     dist.all_gather(gathered, both, group=group)
-    g = np.stack([x.cpu().numpy() for x in gathered])
-    m = slab_merge(np.array([int(c.item()) for c in counts], np.int64), g[:, 0], g[:, 1])
+    g = torch.stack(gathered).cpu().numpy()
+    shape = (world,) + tuple(top.shape)
+    m = slab_merge(g[:, 2 * n].astype(np.int64), g[:, :n].reshape(shape), g[:, n:2 * n].reshape(shape))
     return rank, m
 
 
@@ -81,6 +95,8 @@ def label_distributed(ctx: Context, slab, out, threshold: int = 0, group=None, s
     """Rank k labels slab k (2D rows or 3D planes, on its own GPU), takes part in the exchange and
     maps its labels to the whole image's.  Every rank must call it, with slabs in rank order and
     equal border sizes.  Returns the component count of the whole image."""
+    import torch.distributed as dist
+    _reserve(ctx, tuple(slab.shape), dist.get_world_size(group))
     if slab.dim() == 3:
         count = label3d(ctx, slab, out, threshold=threshold, stream=stream)
     else:

@@ -10,11 +10,16 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def gray_ref(img: np.ndarray, binarize: bool = True, rgb: bool = False) -> np.ndarray:
-    """cv::COLOR_RGB2GRAY on 8-bit data (OpenCV's 14-bit fixed point), then threshold 8."""
+def gray_ref(img: np.ndarray, binarize: bool = True, rgb: bool = False, opencv4: bool = False) -> np.ndarray:
+    """cv::COLOR_RGB2GRAY on 8-bit data, then threshold 8.  OpenCV 3.0.0 (the reference's version)
+    rounds 0.299 / 0.587 / 0.114 with 14-bit weights; OpenCV 4 with 15-bit weights summing to
+    2^15 (tests/test_io_restatement.py pins the latter to the cv2 in this image)."""
     if rgb:
         r, g, b = (img[..., k].astype(np.uint32) for k in range(3))
-        y = (r * 4899 + g * 9617 + b * 1868 + (1 << 13)) >> 14
+        if opencv4:
+            y = (r * 9798 + g * 19235 + b * 3735 + (1 << 14)) >> 15
+        else:
+            y = (r * 4899 + g * 9617 + b * 1868 + (1 << 13)) >> 14
     else:
         y = img.astype(np.uint32)
     return np.where(y > 8, 255, 0).astype(np.uint8) if binarize else y.astype(np.uint8)
@@ -46,6 +51,34 @@ def test_to_gray_matches_rgb2gray(ctx, channels):
         out = torch.empty((333, 517), dtype=torch.uint8, device="cuda")
         be.to_gray(ctx, d, out, binarize=binarize)
         assert np.array_equal(out.cpu().numpy(), gray_ref(img, binarize, channels == 3))
+
+
+@pytest.mark.parametrize("channels", [1, 3])
+def test_to_gray_matches_opencv(ctx, channels):
+    """Pinned to OpenCV itself: the reference's RGB2Gray is cv::cvtColor(COLOR_RGB2GRAY) for
+    colour input, then cv::threshold(img, img, cv::THRESH_OTSU, 255, CV_8UC1) -- THRESH_OTSU (8)
+    passed as the threshold value and CV_8UC1 (0) as the type, THRESH_BINARY
+    (LabelingTools.cpp:39-49)."""
+    import cv2
+    import torch
+    import labeling_b200 as be
+    rng = np.random.default_rng(11 + channels)
+    shape = (301, 419, 3) if channels == 3 else (301, 419)
+    for hi in (40, 256):
+        img = rng.integers(0, hi, shape, dtype=np.uint8)
+        gray = cv2.cvtColor(img, cv2.COLOR_RGB2GRAY) if channels == 3 else img
+        _, want = cv2.threshold(gray, cv2.THRESH_OTSU, 255, cv2.THRESH_BINARY)
+        d = torch.from_numpy(img).cuda()
+        out = torch.empty(shape[:2], dtype=torch.uint8, device="cuda")
+        # the cv2 in this image is OpenCV 4: its weights, bit for bit
+        be.to_gray(ctx, d, out, binarize=True, opencv4=True)
+        assert np.array_equal(out.cpu().numpy(), want)
+        be.to_gray(ctx, d, out, binarize=False, opencv4=True)
+        assert np.array_equal(out.cpu().numpy(), gray)
+        # the default (OpenCV 3.0.0's weights) stays within one gray level of it
+        be.to_gray(ctx, d, out, binarize=False)
+        diff = np.abs(out.cpu().numpy().astype(np.int32) - gray.astype(np.int32))
+        assert diff.max() <= 1 and (channels == 3 or diff.max() == 0)
 
 
 @pytest.mark.parametrize("channels,shape", [(1, (70, 45, 33)), (3, (40, 37, 65)), (1, (1, 1, 1))])

@@ -124,3 +124,29 @@ def test_device_resident_requests():
         ref, kr = _ref(a)
         assert st == 0 and k == kr and np.array_equal(y.cpu().numpy(), ref)
     srv.close()
+
+
+def test_admission_sees_memory_taken_after_creation():
+    """Admission reads the device's free memory when it forms a batch, not only the budget fixed
+    at creation: memory another user of the GPU takes later holds a request back (it stays
+    pending, no failure) until that memory is released."""
+    import torch
+    import labeling_b200 as be
+    from labeling_b200 import workloads as W
+    torch.cuda.empty_cache()
+    srv = be.Server(lanes=1, max_batch=1)          # budget: 80% of the free memory now
+    img = W.bernoulli((4096, 4096), 0.5, 3)         # needs ~117 MB of device memory
+    out = np.zeros(img.shape, np.int32)
+    free, _ = torch.cuda.mem_get_info()
+    hog = torch.empty(max(free - (48 << 20), 0), dtype=torch.uint8, device="cuda")   # leaves ~48 MB
+    try:
+        rid = srv.submit(img, out)
+        st, _, _ = srv.wait(rid, timeout_us=300_000)
+        assert st == 5                              # BE_ERR_TIMEOUT: still waiting for memory
+    finally:
+        del hog
+        torch.cuda.empty_cache()
+    st, k, _ = srv.wait(rid)
+    ref, kr = O.ccl2d(img)
+    assert st == 0 and k == kr and np.array_equal(out, ref)
+    srv.close()

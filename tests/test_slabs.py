@@ -289,3 +289,29 @@ def test_gpu_slab_relabel_odd_pitch_and_offset_only(ctx):
     be.slab_relabel(ctx, view, 3, 4, np.array([2], np.int32), np.array([1], np.int32))
     torch.cuda.synchronize()
     assert base.cpu().tolist() == [[0, 0, 5, 1, 0], [0, 1, 0, 6, 0]]
+
+
+@pytest.mark.gpu
+def test_gpu_label_distributed_one_rank(ctx):
+    """label_distributed over a one-rank NCCL group on one GPU: the packed all_gather of border
+    rows and count on CUDA tensors, the host merge and the relabel call in stream order, against
+    whole-image labels (2D and 3D).  Several ranks need several GPUs."""
+    import socket
+    import torch
+    import torch.distributed as dist
+    from labeling_b200 import workloads as W
+    from labeling_b200.slabs import label_distributed
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        for img in (W.bernoulli((777, 1301), 0.5, seed=41), W.bernoulli((40, 50, 61), 0.3, seed=42)):
+            ref, k = O.ccl2d(img) if img.ndim == 2 else O.ccl3d(img)
+            d = torch.from_numpy(img).cuda()
+            out = torch.full(img.shape, -1, dtype=torch.int32, device="cuda")
+            total = label_distributed(ctx, d, out)
+            assert total == k
+            assert np.array_equal(out.cpu().numpy(), ref)
+    finally:
+        dist.destroy_process_group()

@@ -43,6 +43,34 @@ def test_noalloc_matches_label2d_on_two_calls():
     ctx.close()
 
 
+@pytest.mark.parametrize("shape", [(4096, 4096), (65536, 256)])
+def test_noalloc_at_its_limits(shape):
+    """Images that fill the fixed scratch exactly: 4096 x 4096 is 1024 tiles, 65536 x 256 is 1024
+    tiles and 65536 segments (one per row).  Labels and count must equal be_label2d's; one call
+    passes no count pointer and is followed by a stream synchronization."""
+    import torch
+    import labeling_b200 as be
+    from labeling_b200 import workloads as W
+    f = _noalloc()
+    ctx = be.Context(0)
+    img = W.bernoulli(shape, 0.45, seed=shape[0] % 97)
+    d_in = torch.from_numpy(img).cuda()
+    ref = torch.empty(img.shape, dtype=torch.int32, device="cuda")
+    k_ref = be.label2d(ctx, d_in, ref)
+    stream = torch.cuda.current_stream()
+    for want_count in (True, False):
+        out = torch.full(img.shape, -1, dtype=torch.int32, device="cuda")
+        k = ctypes.c_int64(-1)
+        rc = f(d_in.data_ptr(), img.shape[1], img.shape[0], img.shape[1], 0, out.data_ptr(),
+               img.shape[1], ctypes.byref(k) if want_count else None, stream.cuda_stream)
+        assert rc == 0
+        stream.synchronize()
+        if want_count:
+            assert k.value == k_ref
+        assert torch.equal(out, ref)
+    ctx.close()
+
+
 def test_noalloc_refuses_images_beyond_its_scratch():
     import torch
     f = _noalloc()
