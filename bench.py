@@ -43,7 +43,7 @@ from labeling_b200 import replicas
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-STAGES_2D = ["k_tile_local_2d", "k_merge_2d", "k_post_2d", "k_segscan", "k_tile_write_2d"]
+STAGES_2D = ["k_tile_local_2d", "k_merge_2d", "k_scan_flatten_2d", "k_tile_write_2d"]
 STAGES_3D = ["k_tile_local_3d", "k_merge_3d", "k_post_3d", "k_segscan", "k_tile_write_3d"]
 # Algorithmic bytes per pixel of each launch (what the launch must move at minimum):
 # tile_local reads the image (1 B), tile_write writes the labels (4 B); the others move only
@@ -52,7 +52,7 @@ ALGO_BYTES = {"k_tile_local_2d": 1.0, "k_tile_write_2d": 4.0, "k_tile_local_3d":
               "k_tile_write_3d": 4.0}
 
 # Bytes the union-find pipeline itself moves per pixel / voxel, by array (reads and writes of the
-# five launches, counted from the kernels' loads and stores; node records of border components,
+# pipeline's launches, counted from the kernels' loads and stores; node records of border components,
 # at most a few bytes per border pixel, are left out).  2D tile 64 x 256 px, 3D tile 16 x 32 x 64.
 IMPL_BYTES = {
     "2d": {"input read": 1.0, "labels written": 4.0,
@@ -527,7 +527,7 @@ def bench_plain(args, rank, world, local_rank, workload):
         "config": {**headline_config(workload, [n for n, _ in inputs], inputs[0][1].shape, world),
                    "form": form},
         "e2e": e2e, "roofline": roofline, "roofline_kernels": kernels,
-        "gpu_launches": (5 * steps) if algo == be.ALGO_UF else None, "clocks": clocks,
+        "gpu_launches": (len(stages) * steps) if algo == be.ALGO_UF else None, "clocks": clocks,
         "components": {n: c for (n, _), c in zip(inputs, counts)},
         "per_image_ms": per_image,
         "per_image_stage_ms": {k: [round(float(x), 4) for x in np.mean(v, axis=0)] for k, v in per_stage.items()},
@@ -627,7 +627,7 @@ def bench_batch(args, rank, world, local_rank):
                    "density": "U[0.2, 0.8]", "pixels": npx, "l2": "inputs 1.3 GB > L2",
                    "tuned_choice": choice, "parallelism": f"replicas x{world}"},
         "plain_per_image": {"value": round(plain, 3), "unit": "Gpx/s", "ms": round(plain_ms, 3),
-                            "launches": 5 * n},
+                            "launches": len(STAGES_2D) * n},
         "batched_vs_plain": round(value / world / plain, 2),
         "e2e": {"value": round(npx * e2e_steps / e2e_s / 1e9, 3), "unit": "Gpx/s",
                 "h2d_bytes_per_step": int(npx), "d2h_bytes_per_step": int(4 * npx)},
@@ -635,7 +635,7 @@ def bench_batch(args, rank, world, local_rank):
                      "frac": round(achieved / peak, 4), "traffic": int(sum(IMPL_BYTES["2d"].values()) * npx),
                      "traffic_source": "analytic (as the 2D headline, per pixel)", "peak_kind": peak_kind,
                      "scope": "whole batch (one graph), 5 B/px"},
-        "gpu_launches": 5 * args.steps, "clocks": clk.summary(),
+        "gpu_launches": len(STAGES_2D) * args.steps, "clocks": clk.summary(),
         "components_total": int(sum(counts)),
         "batched_differs_from_plain": len(differ),
     }

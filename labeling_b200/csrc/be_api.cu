@@ -77,12 +77,21 @@ size_t layout_work(const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_img
     t.queue = reinterpret_cast<uint32_t *>(take(kQueueWords * sizeof(uint32_t)));
     t.ncomp = reinterpret_cast<int64_t *>(take(size_t(std::max(n_imgs, 1)) * sizeof(int64_t)));
     t.err = reinterpret_cast<uint32_t *>(take(16 * sizeof(uint32_t)));
+    t.epoch = reinterpret_cast<uint32_t *>(take(2 * sizeof(uint32_t)));
+    t.scan_status = reinterpret_cast<uint64_t *>(take(size_t(std::max<int64_t>(n_chunks, 1)) * sizeof(uint64_t)));
     t.n_tiles = n_tiles;
     t.n_segs = n_segs;
     t.n_chunks = int32_t(n_chunks);
     t.n_imgs = n_imgs;
     if (w) *w = t;
     return off;
+}
+
+cudaError_t reset_scan_state(const Work &w, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(w.epoch, 0, 2 * sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.scan_status, 0, size_t(std::max(w.n_chunks, 1)) * sizeof(uint64_t), s);
+    return e;
 }
 
 int Workspace::ensure(be_ctx *ctx, const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_imgs)
@@ -101,6 +110,10 @@ int Workspace::ensure(be_ctx *ctx, const Geometry &g, int64_t n_tiles, int64_t n
             base = nullptr;
             return cuda_error(ctx, e, "cudaMalloc(workspace)");
         }
+        // The scan's status words and the launch epoch start at zero once; every later run tells
+        // its own status words from older ones by the epoch it increments.
+        e = cudaMemset(base, 0, grow);
+        if (e != cudaSuccess) return cuda_error(ctx, e, "cudaMemset(workspace)");
         bytes = grow;
     }
     layout_work(g, n_tiles, n_segs, n_imgs, static_cast<char *>(base), &w);
@@ -178,7 +191,7 @@ cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persist
         if (e == cudaSuccess) e = r;
     };
     mark(0);
-    k_tile_local_3d<<<grid(w.n_tiles, 5), kT3LocalThreads, 0, s>>>(L, wk);
+    k_tile_local_3d<<<grid(w.n_tiles, 6), kT3LocalThreads, 0, s>>>(L, wk);
     keep(cudaGetLastError());
     mark(1);
     keep(launch_k(k_merge_3d, grid(w.n_tiles, 8), kT3MergeThreads, s, ov, L, wk));
@@ -236,6 +249,10 @@ int be_destroy(be_ctx *c)
     c->ws2d.release();
     c->ws3d.release();
     c->wsiter.release();
+    for (be_iter_graph &g : c->iter_graph) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
     if (c->d_in) cudaFree(c->d_in);
     if (c->d_out) cudaFree(c->d_out);
     if (c->slab_buf) cudaFree(c->slab_buf);
@@ -325,7 +342,7 @@ int be_label2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
         cudaMemsetAsync(c->ws2d.w.err, 0, 16 * sizeof(uint32_t), s);
 #endif
         e = uf2d_launch(shape, L, c->ws2d.w, c->sms, false, s, c->timing ? c->stage_ev : nullptr);
-        c->timed_stages = c->timing ? kStages : 0;
+        c->timed_stages = c->timing ? kStages2D : 0;
         if (e != cudaSuccess) return cuda_error(c, e, "be_label2d launch");
     }
     if (rc) return rc;

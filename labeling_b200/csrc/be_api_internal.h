@@ -32,6 +32,8 @@ cudaError_t uf2d_launch(int shape, const ImgList2D &L, const Work &w, int sms, b
 Geometry geometry_2d();   // shape 0
 Geometry geometry_3d();
 size_t layout_work(const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_imgs, char *base, Work *w);
+// Zeroes a workspace's launch epoch and scan status words (memory that was not zeroed before).
+cudaError_t reset_scan_state(const Work &w, cudaStream_t s);
 
 // One growable device allocation holding a Work.
 struct Workspace {
@@ -68,7 +70,8 @@ void fill_img2d(Img2D &im, const uint8_t *in, int64_t in_pitch, int32_t rows, in
                 int shape = 0);
 void fill_img3d(Img3D &im, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int thr,
                 int32_t *out, int64_t tile_base, int64_t seg_base, int index);
-constexpr int kStages = 5;   // launches of one union-find pipeline
+constexpr int kStages = 5;     // launches of the 3D union-find pipeline (the most of any form)
+constexpr int kStages2D = 4;   // launches of the 2D union-find pipeline
 cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persistent, cudaStream_t s,
                         cudaEvent_t *ev = nullptr);
 
@@ -82,6 +85,14 @@ int run_lbeq3d(struct ::be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, in
                int32_t *out, cudaStream_t s);
 
 }  // namespace be
+
+// An instantiated graph of the iterative form, kept for the next call of the same form and sizes.
+struct be_iter_graph {
+    std::vector<unsigned char> key;   // the graph's baked-in arguments, image buffers blanked
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphNode_t init = nullptr, fin = nullptr;   // the nodes that read / write the image
+};
 
 struct be_ctx {
     int device = 0;
@@ -103,4 +114,5 @@ struct be_ctx {
     cudaEvent_t stage_ev[be::kStages + 1] = {};
     std::vector<be::TuneEntry> tune;  // autotuner decisions
     int last_algo = 1;                // algorithm the last label call actually ran
+    be_iter_graph iter_graph[4];      // iterative form: 2D / 3D blocks, 2D / 3D pixels
 };

@@ -84,6 +84,8 @@ int build(be_batch *b)
         return cuda_error(c, e, "be_batch: cudaMalloc");
     }
     b->dev_bytes = total;
+    e = cudaMemset(b->dev, 0, total);   // scan status words and launch epochs start at zero
+    if (e != cudaSuccess) return cuda_error(c, e, "be_batch: cudaMemset");
     char *base = static_cast<char *>(b->dev);
     b->counts = reinterpret_cast<int64_t *>(base + o_cnt);
     if (!d2.empty()) e = cudaMemcpy(base + o_d2, d2.data(), d2.size() * sizeof(Img2D), cudaMemcpyHostToDevice);

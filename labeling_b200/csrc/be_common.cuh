@@ -75,6 +75,8 @@ struct Work {
     uint32_t *queue;      // work-queue counters (persistent mode); zeroed before a launch
     int64_t *ncomp;       // per image: number of components
     uint32_t *err;        // error flags (bounded waits / iteration caps)
+    uint32_t *epoch;      // [0] launch epoch (+1 per pipeline run), [1] scan ticket counter
+    uint64_t *scan_status;  // per scan chunk: (epoch << 34 | state << 32) | prefix value
     int64_t n_tiles;
     int64_t n_segs;
     int32_t n_chunks;
@@ -263,6 +265,22 @@ __device__ __forceinline__ void gunion_keyed(uint32_t *gp, const uint32_t *nkey,
         pa = old;
         pb = vp[b];
     }
+}
+
+// Find with path halving after all merges of the launch are complete: no link can happen any more,
+// so every pointer stored is to an ancestor and any interleaving of the stores keeps the trees
+// valid.  The cap only bounds the walk should the forest ever hold a cycle (it cannot).
+__device__ __forceinline__ uint32_t gfind_halve(uint32_t *gp, uint32_t a)
+{
+    volatile uint32_t *vp = gp;
+    uint32_t p = vp[a];
+    for (int it = 0; p != a && it < (1 << 24); ++it) {
+        const uint32_t g = vp[p];
+        if (g != p) vp[a] = g;
+        a = p;
+        p = g;
+    }
+    return a;
 }
 
 // Read-only find (after all merges of the launch are complete).

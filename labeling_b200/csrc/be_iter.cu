@@ -22,6 +22,7 @@
 #include "be_kernels.h"
 
 #include <algorithm>
+#include <cstring>
 
 namespace be {
 
@@ -563,15 +564,60 @@ int iter_scratch(be_ctx *c, int64_t nblocks, size_t conn_bytes, int64_t nwords, 
     return BE_OK;
 }
 
+// The arguments that only the init and final kernels read (the image buffers and threshold),
+// blanked for the graph cache's key.
+void blank_io(It2 &g) { g.in = nullptr; g.out = nullptr; g.pitch = g.opitch = 0; g.thr = 0; }
+void blank_io(It3 &g) { g.in = nullptr; g.out = nullptr; g.thr = 0; }
+void blank_io(Lq2 &g) { g.in = nullptr; g.out = nullptr; g.pitch = g.opitch = 0; g.thr = 0; }
+void blank_io(Lq3 &g) { g.in = nullptr; g.out = nullptr; g.thr = 0; }
+
+template <class G>
+cudaError_t set_kernel_args(cudaGraphExec_t exec, cudaGraphNode_t node, void *fn, unsigned grid, G &g)
+{
+    void *argv[] = {static_cast<void *>(&g)};
+    cudaKernelNodeParams p = {};
+    p.func = fn;
+    p.gridDim = dim3(std::max(grid, 1u));
+    p.blockDim = dim3(NT);
+    p.sharedMemBytes = 0;
+    p.kernelParams = argv;
+    return cudaGraphExecKernelNodeSetParams(exec, node, &p);
+}
+
 // Builds and launches the graph: memsets, init, conn, WHILE{scan, analyze, cond}, mark, count,
-// chunk sums, segment scan, final, count/flag copy-out.
+// chunk sums, segment scan, final, count/flag copy-out.  The instantiated graph is kept in the
+// context (one per form) and launched again, with only the init and final nodes' arguments
+// updated, while the sizes and scratch buffers stay the same.
 template <class G, class FI, class FC, class FS, class FA, class FM, class FF>
-int run_graph(be_ctx *c, G g, int64_t nblocks, int64_t nfinal, int64_t nwords, FI f_init, FC f_conn,
+int run_graph(be_ctx *c, int kind, G g, int64_t nblocks, int64_t nfinal, int64_t nwords, FI f_init, FC f_conn,
               FS f_scan, FA f_an, FM f_mark, FF f_final, cudaStream_t s)
 {
+    be_iter_graph &cache = c->iter_graph[kind];
+    std::vector<unsigned char> key(sizeof(G) + 4 * sizeof(int64_t));
+    {
+        G k;
+        std::memcpy(&k, &g, sizeof(G));
+        blank_io(k);
+        std::memcpy(key.data(), &k, sizeof(G));
+        const int64_t extra[4] = {nblocks, nfinal, nwords, int64_t(reinterpret_cast<uintptr_t>(c->iter_err))};
+        std::memcpy(key.data() + sizeof(G), extra, sizeof(extra));
+    }
+    cudaError_t e;
+    if (cache.exec && cache.key == key) {
+        e = set_kernel_args(cache.exec, cache.init, reinterpret_cast<void *>(f_init), nblk(nblocks), g);
+        if (e == cudaSuccess)
+            e = set_kernel_args(cache.exec, cache.fin, reinterpret_cast<void *>(f_final), nblk(nfinal), g);
+        if (e == cudaSuccess) e = cudaGraphLaunch(cache.exec, s);
+        if (e != cudaSuccess) return cuda_error(c, e, "iterative graph (cached)");
+        return BE_OK;
+    }
+    if (cache.exec) cudaGraphExecDestroy(cache.exec);
+    if (cache.graph) cudaGraphDestroy(cache.graph);
+    cache = be_iter_graph{};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    cudaError_t e = cudaGraphCreate(&graph, 0);
+    cudaGraphNode_t n_init = nullptr, n_final = nullptr;
+    e = cudaGraphCreate(&graph, 0);
     if (e != cudaSuccess) return cuda_error(c, e, "cudaGraphCreate");
     cudaGraphNode_t n = nullptr, prev = nullptr;
     auto chain = [&](cudaError_t err) {
@@ -595,6 +641,7 @@ int run_graph(be_ctx *c, G g, int64_t nblocks, int64_t nfinal, int64_t nwords, F
         e = chain(cudaGraphAddMemsetNode(&n, graph, &prev, 1, &m2));
     }
     if (e == cudaSuccess) e = chain(add_kernel(graph, &n, prev, f_init, nblk(nblocks), NT, g));
+    if (e == cudaSuccess) n_init = n;
     if (e == cudaSuccess && f_conn) e = chain(add_kernel(graph, &n, prev, f_conn, nblk(nblocks), NT, g));
     cudaGraphConditionalHandle h;
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
@@ -622,6 +669,7 @@ int run_graph(be_ctx *c, G g, int64_t nblocks, int64_t nfinal, int64_t nwords, F
     if (e == cudaSuccess)
         e = chain(add_kernel(graph, &n, prev, k_segscan, unsigned(g.w.n_chunks), unsigned(kScanThreads), g.w));
     if (e == cudaSuccess) e = chain(add_kernel(graph, &n, prev, f_final, nblk(nfinal), NT, g));
+    if (e == cudaSuccess) n_final = n;
     if (e == cudaSuccess)
         e = chain(add_kernel(graph, &n, prev, it_ncomp, 1u, 1u, g.w, (const uint32_t *)g.ctl, g.ctl + 3));
     if (e == cudaSuccess) {
@@ -634,9 +682,16 @@ int run_graph(be_ctx *c, G g, int64_t nblocks, int64_t nfinal, int64_t nwords, F
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
-    if (exec) cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return cuda_error(c, e, "iterative graph");
+    if (e != cudaSuccess) {
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        return cuda_error(c, e, "iterative graph");
+    }
+    cache.key = std::move(key);
+    cache.graph = graph;
+    cache.exec = exec;
+    cache.init = n_init;
+    cache.fin = n_final;
     return BE_OK;
 }
 
@@ -665,7 +720,7 @@ int run_iter2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
     g.w = c->wsiter.w;
     g.w.n_tiles = 0;
     g.w.queue = nullptr;
-    return run_graph(c, g, nblocks, int64_t(g.bw) * rows, nwords, it_init_2d, it_conn_2d, it_scan_2d,
+    return run_graph(c, 0, g, nblocks, int64_t(g.bw) * rows, nwords, it_init_2d, it_conn_2d, it_scan_2d,
                      it_analyze_2d, it_mark_2d, it_final_2d, s);
 }
 
@@ -691,7 +746,7 @@ int run_iter3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
     g.w = c->wsiter.w;
     g.w.n_tiles = 0;
     g.w.queue = nullptr;
-    return run_graph(c, g, nblocks, int64_t(d0) * d1 * d2, nwords, it_init_3d, it_conn_3d, it_scan_3d,
+    return run_graph(c, 1, g, nblocks, int64_t(d0) * d1 * d2, nwords, it_init_3d, it_conn_3d, it_scan_3d,
                      it_analyze_3d, it_mark_3d, it_final_3d, s);
 }
 
@@ -716,7 +771,7 @@ int run_lbeq2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
     g.w = c->wsiter.w;
     g.w.n_tiles = 0;
     g.w.queue = nullptr;
-    return run_graph(c, g, n, n, nwords, lq_init_2d, (void (*)(Lq2)) nullptr, lq_scan_2d, lq_analyze_2d,
+    return run_graph(c, 2, g, n, n, nwords, lq_init_2d, (void (*)(Lq2)) nullptr, lq_scan_2d, lq_analyze_2d,
                      lq_mark_2d, lq_final_2d, s);
 }
 
@@ -740,7 +795,7 @@ int run_lbeq3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
     g.w = c->wsiter.w;
     g.w.n_tiles = 0;
     g.w.queue = nullptr;
-    return run_graph(c, g, n, n, nwords, lq_init_3d, (void (*)(Lq3)) nullptr, lq_scan_3d, lq_analyze_3d,
+    return run_graph(c, 3, g, n, n, nwords, lq_init_3d, (void (*)(Lq3)) nullptr, lq_scan_3d, lq_analyze_3d,
                      lq_mark_3d, lq_final_3d, s);
 }
 

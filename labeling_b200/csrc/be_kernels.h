@@ -26,6 +26,7 @@ __global__ void k_post_3d(ImgList3D L, Work w);
 __global__ void k_tile_write_3d(ImgList3D L, Work w);
 
 __global__ void k_segscan(Work w);
+__global__ void k_segscan_lb(Work w);
 __global__ void k_chunk_sums(Work w);
 
 constexpr int kPostThreads = 128;

@@ -12,8 +12,10 @@
 // The array's name is only a stand-in in host code; the kernels receive the device address that
 // cudaGetSymbolAddress returns, looked up once per device (with that device current) on the
 // first call there.  All calls share the one array, so calls whose work overlaps on the GPU (other
-// streams, other host threads) race: the caller must order them.  Nothing in the pipeline needs the
-// scratch to start at zero: every launch writes each scratch word it later reads.
+// streams, other host threads) race: the caller must order them.  Nothing needs clearing between
+// calls: every launch writes each scratch word it later reads, except the segment scan's status
+// words, which carry the number of the call that wrote them (a counter in the array that each call
+// increments), so words left by earlier calls are ignored; the array is zero when the library loads.
 #include "be.h"
 #include "be_api_internal.h"
 #include "be_kernels.h"
@@ -38,7 +40,8 @@ constexpr size_t kScratchBytes =
     al256((kMaxSegs + 15) / 16 * 16 + 16) +                       // segment counts
     al256((kMaxSegs + 1) * 4) +                                   // segment prefix
     al256(((kMaxSegs + be::kScanChunk - 1) / be::kScanChunk) * 4) +
-    al256(be::kQueueWords * 4) + al256(8) + al256(64) + 4096;     // queue, count, flags, slack
+    al256(be::kQueueWords * 4) + al256(8) + al256(64) +           // queue, count, flags
+    al256(8) + al256(((kMaxSegs + be::kScanChunk - 1) / be::kScanChunk) * 8) + 4096;   // scan state, slack
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 

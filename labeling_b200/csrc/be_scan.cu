@@ -1,5 +1,6 @@
-// be_scan.cu -- exclusive scan of the per-segment root counts (second half of the two-launch
-// scan; the first half, the chunk sums, runs inside k_post_2d / k_post_3d).
+// be_scan.cu -- exclusive scan of the per-segment root counts: k_segscan is the second half of
+// the two-launch scan (the chunk sums run inside k_post_3d, or k_chunk_sums), k_segscan_lb the
+// single-pass form of the 2D pipeline.
 #include "be_kernels.h"
 #include "be_scan.cuh"
 
@@ -9,6 +10,9 @@ namespace be {
 // counts and writes segpref[i] = sum of segcnt[0, i).  The last chunk also writes segpref[n_segs].
 __global__ void __launch_bounds__(kScanThreads) k_segscan(Work w)
 {
+    // The release comes after the wait on purpose: the label-write launch that follows reads the
+    // post-merge pass's results before its own wait, which is safe only because this grid lets it
+    // start once that pass has completed.
     grid_dep_wait();
     grid_dep_release();
     constexpr int NT = kScanThreads;
@@ -57,6 +61,17 @@ __global__ void __launch_bounds__(kScanThreads) k_segscan(Work w)
         }
     }
     if (c == gridDim.x - 1 && threadIdx.x == 0) w.segpref[w.n_segs] = off + ctot;
+}
+
+// Single-pass scan of the segment counts (one CTA per chunk; see segscan_lb_chunk).
+__global__ void __launch_bounds__(kScanThreads) k_segscan_lb(Work w)
+{
+    // Release after the wait, as k_segscan: the label-write launch relies on it.
+    grid_dep_wait();
+    grid_dep_release();
+    __shared__ uint32_t tmp[kScanThreads / 32 + 1];
+    __shared__ uint32_t sh[2];
+    segscan_lb_chunk<kScanThreads>(w, tmp, sh);
 }
 
 // Chunk sums alone (one CTA per chunk), for pipelines without border roots to rank.

@@ -249,6 +249,7 @@ bool be_server::launch(Lane &ln, std::vector<Req *> &batch)
         layout_work(g2, t2, s2, nimg, base + o_w2, &W);
         W.ncomp = counts;
         cudaMemsetAsync(W.queue, 0, kQueueWords * sizeof(uint32_t), s);
+        reset_scan_state(W, s);   // the pool's memory is not zeroed
         ImgList2D L{reinterpret_cast<const Img2D *>(base), int(ln.d2.size()), ln.d2[0]};
         le = uf2d_launch(0, L, W, sms, true, s);
     }
@@ -257,6 +258,7 @@ bool be_server::launch(Lane &ln, std::vector<Req *> &batch)
         layout_work(g3, t3, s3, nimg, base + o_w3, &W);
         W.ncomp = counts;
         cudaMemsetAsync(W.queue, 0, kQueueWords * sizeof(uint32_t), s);
+        reset_scan_state(W, s);
         ImgList3D L{reinterpret_cast<const Img3D *>(base + o_d3), int(ln.d3.size()), ln.d3[0]};
         le = launch_uf3d(L, W, sms, true, s);
     }

@@ -3,16 +3,19 @@
 // (32 x 128, 64 x 64 and 16 x 256 blocks) that the autotuner chooses between.
 //
 // Replaces the reference's LBEQ2_Init / LBEQ2_Scan / LBEQ2_Analyze / LBEQ2_SetFinalLabels
-// (LabelingAlgs.cl:176-319) and their host loop (LabelingAlgs.cpp:989-1084) with five launches:
+// (LabelingAlgs.cl:176-319) and their host loop (LabelingAlgs.cpp:989-1084) with four launches:
 //
 //   k_tile_local_2d   one CTA per 64x256-pixel tile: 16-byte coalesced loads, 2x2 block masks,
-//                     block union-find in shared memory (atomicMin, smaller key wins), flatten,
+//                     runs of blocks and their links by bit operations; each run's first link
+//                     becomes its parent by a plain store (a forest, flattened by pointer jumping),
+//                     the other links are atomicMin unions in shared memory (smaller key wins);
 //                     write one uint16 per block = (mask << 12) | tile-local root block; count
-//                     roots per segment; export border components as nodes.
+//                     roots per segment; mark each component's first pixel in the tile's root
+//                     bitmap; export border components as nodes.
 //   k_merge_2d        unions nodes across tile borders (global union-find, smaller key wins);
-//                     every root that gets linked is removed from its segment count.
-//   k_post            (be_scan.cu) ranks of surviving border roots + scan-chunk sums.
-//   k_segscan         (be_scan.cu) exclusive scan of the segment counts.
+//                     every root that gets linked leaves its segment count and its root bitmap.
+//   k_scan_flatten_2d single-pass exclusive scan of the segment counts (be_scan.cuh) and, in
+//                     the same launch, every linked node pointed straight at its global root.
 //   k_tile_write_2d   one CTA per tile: resolves each block's canonical label and writes the int32
 //                     labels with 16-byte stores.
 //

@@ -9,7 +9,7 @@ constexpr int NPERIM = 2 * (TBW + TBH);            // border positions per tile
 constexpr int MAXB = NPERIM;                       // nodes per tile
 constexpr int WPR = TBW / 32;                      // 32-block words per block row
 constexpr int K1_NT = TBH * WPR;                   // one thread per (block row, word) = NBLK / 32
-constexpr int MQCAP = 2816;                        // merge-queue capacity (more merge in place)
+constexpr int MQCAP = 1024;                        // union-queue capacity (more merge in place)
 constexpr uint32_t kPass = 0xFFFFu;                // "no run start" in the carry scan
 
 static_assert(NBLK <= 4096, "tile-local block index must fit 12 bits");
@@ -69,17 +69,22 @@ __device__ __forceinline__ uint32_t spread4(uint32_t x) { return ((x & 0xFu) * 0
 // Highest set bit of x (x != 0).
 __device__ __forceinline__ uint32_t hibit(uint32_t x) { return 31u - __clz(x); }
 
+// Shared-memory position of block x's union-find entry: the low five bits are XOR-ed with the
+// block's 32-block word, so that the 32 lanes of a warp -- 32 different words walking the same
+// bit position -- reach 32 different banks.  Entries still name blocks by their plain index.
+__device__ __forceinline__ uint32_t sw(uint32_t x) { return x ^ ((x >> 5) & 31u); }
+
 // Union-find over run starts with the slot order carried in the parent entry: P[x] holds
 // (slot << 12) | parent, and a root holds its own (slot << 12) | x.  Entries only ever decrease,
 // so the union (atomicMin of the smaller encoding into the other root, Playne-Hawick style)
 // leaves the run with the smallest slot -- the component's first pixel -- as the root.
 __device__ __forceinline__ uint32_t efind(uint32_t *P, uint32_t x)
 {
-    uint32_t v = P[x];
+    uint32_t v = P[sw(x)];
     while ((v & 0xFFFu) != x) {
         const uint32_t y = v & 0xFFFu;
-        const uint32_t vg = P[y];
-        if ((vg & 0xFFFu) != y) P[x] = vg;   // path halving
+        const uint32_t vg = P[sw(y)];
+        if ((vg & 0xFFFu) != y) P[sw(x)] = vg;   // path halving
         x = y;
         v = vg;
     }
@@ -88,10 +93,10 @@ __device__ __forceinline__ uint32_t efind(uint32_t *P, uint32_t x)
 
 __device__ __forceinline__ uint32_t efind_ro(const uint32_t *P, uint32_t x)
 {
-    uint32_t v = P[x];
+    uint32_t v = P[sw(x)];
     while ((v & 0xFFFu) != x) {
         x = v & 0xFFFu;
-        v = P[x];
+        v = P[sw(x)];
     }
     return x;
 }
@@ -99,11 +104,11 @@ __device__ __forceinline__ uint32_t efind_ro(const uint32_t *P, uint32_t x)
 // As efind, also returning the root's own entry as read (the union compares the two).
 __device__ __forceinline__ uint32_t efind_e(uint32_t *P, uint32_t x, uint32_t &ev)
 {
-    uint32_t v = P[x];
+    uint32_t v = P[sw(x)];
     while ((v & 0xFFFu) != x) {
         const uint32_t y = v & 0xFFFu;
-        const uint32_t vg = P[y];
-        if ((vg & 0xFFFu) != y) P[x] = vg;
+        const uint32_t vg = P[sw(y)];
+        if ((vg & 0xFFFu) != y) P[sw(x)] = vg;
         x = y;
         v = vg;
     }
@@ -119,11 +124,11 @@ __device__ __forceinline__ void eunion(uint32_t *P, uint32_t a, uint32_t b)
         b = efind_e(P, b, eb);
         if (a == b) return;
         if (ea < eb) {
-            const uint32_t old = atomicMin(&P[b], ea);
+            const uint32_t old = atomicMin(&P[sw(b)], ea);
             if ((old & 0xFFFu) == b) return;
             b = old & 0xFFFu;
         } else {
-            const uint32_t old = atomicMin(&P[a], eb);
+            const uint32_t old = atomicMin(&P[sw(a)], eb);
             if ((old & 0xFFFu) == a) return;
             a = old & 0xFFFu;
         }
@@ -139,16 +144,20 @@ __device__ __forceinline__ void eunion(uint32_t *P, uint32_t a, uint32_t b)
 // operations; only runs enter the union-find, and only links between runs that no earlier link
 // already joins are merged.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
+__global__ void __launch_bounds__(K1_NT, 7) k_tile_local_2d(ImgList2D L, Work w)
 {
     grid_dep_release();   // the merge launch may take free SMs during this grid's last wave
+    if (blockIdx.x == 0 && threadIdx.x == 0) {   // a new epoch for the segment scan of this run
+        w.epoch[0] += 1u;
+        w.epoch[1] = 0u;
+    }
     __shared__ uint32_t P[NBLK];            // run starts: (slot << 12) | parent
     __shared__ __align__(16) uint8_t M[NBLK];
     __shared__ uint32_t WBL[NBLK / 32], WBR[NBLK / 32], WHC[NBLK / 32], WS[NBLK / 32], WCS[NBLK / 32];
     __shared__ uint32_t RB[TH][TW / 32];
     __shared__ uint32_t BF[NBLK / 32];
     __shared__ uint32_t BP[NBLK / 32];
-    __shared__ uint32_t MQ[MQCAP];          // merge queue: (start_a << 16) | start_b
+    __shared__ uint32_t MQ[MQCAP];          // union queue: (block_a << 16) | block_b
     __shared__ uint32_t mqn;
     __shared__ uint32_t tmp[K1_NT / 32 + 1];
     __shared__ uint32_t qslot;
@@ -261,7 +270,7 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
                 const uint32_t tm = Tw & from & ((2u << e) - 1u);
                 const uint32_t key = tm ? sbase + 32 * q + (__ffs(tm) - 1) : sbase + TBW + 32 * q + s0;
                 const uint32_t x = rbase + 32 * q + s0;
-                P[x] = (key << 12) | x;
+                P[sw(x)] = (key << 12) | x;
             }
         }
         __syncthreads();
@@ -272,7 +281,7 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
             const uint32_t tm = Tw & ((2u << e) - 1u);
             if (tm && GUARD(w, CSc < uint32_t(TBW), 111, CSc)) {
                 const uint32_t x = rbase + (CSc & (TBW - 1));
-                atomicMin(&P[x], ((sbase + 32 * q + (__ffs(tm) - 1)) << 12) | x);
+                atomicMin(&P[sw(x)], ((sbase + 32 * q + (__ffs(tm) - 1)) << 12) | x);
             }
         }
         __syncthreads();   // slots final before any union reads them
@@ -285,10 +294,9 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
         uint32_t Nm = 0, NWm = 0, NEm = 0;
         if (r > 0 && r < nbr) {
             const int u = tid - WPR;   // same word, row above
-            const uint32_t uBL = WBL[u], uBR = WBR[u], uhc = WHC[u];
+            const uint32_t uBL = WBL[u], uBR = WBR[u];
             const uint32_t uBRp = q > 0 ? WBR[u - 1] >> 31 : 0u;
             const uint32_t uBLn = q + 1 < WPR ? WBL[u + 1] & 1u : 0u;
-            const uint32_t uhl = (uhc << 1) | (q > 0 ? WHC[u - 1] >> 31 : 0u);
             const uint32_t N = Tw & (uBL | uBR);
             const uint32_t NW = TLw & ((uBR << 1) | uBRp);
             const uint32_t NE = TRw & ((uBL >> 1) | (uBLn << 31));
@@ -310,11 +318,8 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
                 NEm = NE & ~((N & uhc) | (hl & NEsh & uhc));
             }
         }
-        const uint32_t n = __popc(Nm) + __popc(NWm) + __popc(NEm);
-        uint32_t pos = warp_reserve(&mqn, n);
-        // The queue holds the two blocks of each link; their run starts (a start in the block's
-        // word at or before it, else the start carried in from the left) are looked up by the
-        // merging lanes, which share that work evenly.
+        // The run start of a block: a start in the block's word at or before it, else the start
+        // carried in from the left.
         auto start_of = [&](uint32_t blk) -> uint32_t {
             const uint32_t m = WS[blk >> 5] & ((2u << (blk & 31u)) - 1u);
             const uint32_t st = m ? (blk & ~31u) + hibit(m) : (blk & ~uint32_t(TBW - 1)) + WCS[blk >> 5];
@@ -323,8 +328,45 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
             GUARD(w, st < uint32_t(NBLK), 112, (uint64_t(blk) << 32) | st);
             return st & (NBLK - 1);
         };
+        const uint32_t ubase = rbase - TBW + 32 * q, abase = rbase + 32 * q;
+
+        // Forest: a run that starts in this word takes its first kept link in this word as its
+        // parent.  The parent is in the row above, whose slots are all smaller than this row's, so
+        // a plain store links it (no atomic, no cycle possible).  The parent's entry copied here
+        // is its own root entry or, when its owner has already linked it the same way, the entry
+        // of its own parent: an ancestor either way.  These links leave the queue; the union-find
+        // below walks the forest's paths like any other (path halving), and the flatten pass
+        // compresses them.  (Pointer jumping over the forest first was measured slower.)
         {
-            const uint32_t ubase = rbase - TBW + 32 * q, abase = rbase + 32 * q;
+            uint32_t ss = S;
+            while (ss) {
+                const uint32_t s0 = __ffs(ss) - 1;
+                ss &= ss - 1;
+                const uint32_t brk = ~hc & (~0u << s0);
+                const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
+                const uint32_t lk = (Nm | NWm | NEm) & (~0u << s0) & (0xFFFFFFFFu >> (31u - e));
+                if (!lk) continue;
+                const uint32_t b = __ffs(lk) - 1, bit = 1u << b;
+                uint32_t tgt;
+                if (Nm & bit) {
+                    tgt = ubase + b;
+                    Nm &= ~bit;
+                } else if (NWm & bit) {
+                    tgt = ubase + b - 1;
+                    NWm &= ~bit;
+                } else {
+                    tgt = ubase + b + 1;
+                    NEm &= ~bit;
+                }
+                P[sw(abase + s0)] = P[sw(start_of(tgt))];
+            }
+        }
+        __syncthreads();
+        // The remaining links are unions.  The queue holds the two blocks of each link; their run
+        // starts are looked up by the merging lanes, which share that work evenly.
+        const uint32_t n = __popc(Nm) + __popc(NWm) + __popc(NEm);
+        uint32_t pos = warp_reserve(&mqn, n);
+        {
             auto push = [&](uint32_t a, uint32_t b) {
                 if (pos < uint32_t(MQCAP)) MQ[pos] = (a << 16) | b;
                 else eunion(P, start_of(a), start_of(b));   // queue full: merge in place
@@ -351,35 +393,23 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
         }
         __syncthreads();
 
-        // Phase C: every run start points straight at its root; roots mark their first pixel.
-        // The starts are listed first (the merge queue is free again) and taken round robin, so
-        // the work is even over the lanes and a row's parents -- the row above, listed one
-        // round earlier -- are mostly already compressed when a row is walked.
-        // The list is 16-bit (block indices) in the queue's memory: it holds every block.
-        static_assert(2 * MQCAP >= NBLK, "the run list must hold every block of a tile");
-        uint16_t *runs = reinterpret_cast<uint16_t *>(MQ);
-        if (tid == 0) mqn = 0;
-        __syncthreads();
+        // Phase C: every run start of this word, and every entry on its path, points straight at
+        // its root (a read-only walk, then the root's entry stored along the path: every writer
+        // stores the same final entry, and no link happens any more); roots mark their first
+        // pixel.  Then the block entries: (mask << 12) | root block, two blocks per 32-bit word.
         {
-            uint32_t pos = warp_reserve(&mqn, __popc(S));
             uint32_t ss = S;
             while (ss) {
-                const uint32_t s0 = __ffs(ss) - 1;
+                const uint32_t x = abase + (__ffs(ss) - 1);
                 ss &= ss - 1;
-                runs[pos++] = uint16_t(rbase + 32 * q + s0);
-            }
-        }
-        __syncthreads();
-        {
-            const uint32_t nruns = mqn;
-            for (uint32_t i = tid; i < nruns; i += K1_NT) {
-                const uint32_t x = runs[i];
-                const uint32_t root = efind_ro(P, x);
-                const uint32_t ev = P[root];
-                // Point the whole path at the root (every writer stores the same final value).
-                for (uint32_t y = x; y != root;) {
-                    const uint32_t ny = P[y] & 0xFFFu;
-                    P[y] = ev;
+                uint32_t root = x, ev = P[sw(x)];
+                for (int it = 0; (ev & 0xFFFu) != root && it < NBLK; ++it) {   // acyclic: the cap never binds
+                    root = ev & 0xFFFu;
+                    ev = P[sw(root)];
+                }
+                for (uint32_t y = x, it = 0; y != root && it < NBLK; ++it) {
+                    const uint32_t ny = P[sw(y)] & 0xFFFu;
+                    P[sw(y)] = ev;
                     y = ny;
                 }
                 if (root == x) {
@@ -392,23 +422,30 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
                 }
             }
         }
-        __syncthreads();
-        // Block entries (mask << 12) | root block, two blocks per 32-bit word.
         {
-            uint32_t cur = cin ? key_block(P[rbase + (CSc & (TBW - 1))] >> 12) : 0u;
+            uint32_t cur = 0;
+            if (cin) {   // the run carried in from the left starts in an earlier word of this row
+                uint32_t root = rbase + (CSc & (TBW - 1)), ev = P[sw(root)];
+                for (int it = 0; (ev & 0xFFFu) != root && it < NBLK; ++it) {
+                    root = ev & 0xFFFu;
+                    ev = P[sw(root)];
+                }
+                cur = key_block(ev >> 12);
+            }
             uint32_t ew[16];
 #pragma unroll
             for (int k = 0; k < 32; ++k) {
-                if ((S >> k) & 1u) cur = key_block(P[rbase + 32 * q + k] >> 12);
+                if ((S >> k) & 1u) cur = key_block(P[sw(abase + k)] >> 12);
                 const uint32_t m = (mw[k >> 2] >> (8 * (k & 3))) & 15u;
                 const uint32_t e = m ? (m << 12) | cur : 0u;
                 if (k & 1) ew[k >> 1] |= e << 16;
                 else ew[k >> 1] = e;
             }
-            uint4 *dst = reinterpret_cast<uint4 *>(lab + t * NBLK + rbase + 32 * q);
+            uint4 *dst = reinterpret_cast<uint4 *>(lab + t * NBLK + abase);
 #pragma unroll
             for (int i = 0; i < 4; ++i) dst[i] = make_uint4(ew[4 * i], ew[4 * i + 1], ew[4 * i + 2], ew[4 * i + 3]);
         }
+        __syncthreads();   // root bitmap complete; every run start points at its root
 
         // Phase D: root bitmap and segment counts out; border components -> nodes.
         for (int i = tid; i < TH * (TW / 32); i += K1_NT) w.rbits[t * (TH * (TW / 32)) + i] = (&RB[0][0])[i];
@@ -418,7 +455,10 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
             for (int k = 0; k < TW / 32; ++k) cnt += __popc(RB[tid][k]);
             w.segcnt[im.seg_base + int64_t(y0 + tid) * im.tiles_x + tx] = uint8_t(cnt);
         }
-        uint32_t prb[(NPERIM + K1_NT - 1) / K1_NT];   // root block of each border position held
+        // Root block of each border position held (plus its mask, and whether this position
+        // claimed the node: the one position that sets the root's bit writes the node's record).
+        constexpr uint32_t kOwner = 1u << 20;
+        uint32_t prb[(NPERIM + K1_NT - 1) / K1_NT];
 #pragma unroll
         for (int i = 0; i < (NPERIM + K1_NT - 1) / K1_NT; ++i) {
             const int p = tid + i * K1_NT;
@@ -431,35 +471,37 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
             const uint32_t sm = WS[wi] & ((2u << (bc & 31)) - 1u);
             const uint32_t sc = sm ? uint32_t(bc & ~31) + hibit(sm) : WCS[wi];
             GUARD(w, sc < uint32_t(TBW), 113, sc);
-            const uint32_t rb = key_block(P[uint32_t(br) * TBW + (sc & (TBW - 1))] >> 12);
-            prb[i] = rb | (m << 16);
-            atomicOr(&BF[rb >> 5], 1u << (rb & 31));
+            const uint32_t rb = key_block(P[sw(uint32_t(br) * TBW + (sc & (TBW - 1)))] >> 12);
+            const uint32_t bit = 1u << (rb & 31);
+            const uint32_t old = atomicOr(&BF[rb >> 5], bit);
+            prb[i] = rb | (m << 16) | ((old & bit) ? 0u : kOwner);
         }
         __syncthreads();
         uint32_t nb;
         const uint32_t pre = block_exscan<K1_NT>(__popc(BF[tid]), tmp, &nb);
         BP[tid] = pre;
         __syncthreads();
-        // Every border position writes its entry and (redundantly, with identical values) the
-        // record of the node its root belongs to, which spreads the node work over the CTA.
+            // Every border position writes its entry; the position that claimed its node writes the
+        // node's record.
 #pragma unroll
         for (int i = 0; i < (NPERIM + K1_NT - 1) / K1_NT; ++i) {
             const int p = tid + i * K1_NT;
             if (p >= NPERIM) continue;
             uint16_t ent = 0;
             if (prb[i] != kNone) {
-                const uint32_t rb = prb[i] & 0xFFFFu, m = prb[i] >> 16;
+                const uint32_t rb = prb[i] & 0xFFFFu, m = (prb[i] >> 16) & 15u;
                 const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
                 ent = uint16_t((j << 4) | m);
+            }
+            if (prb[i] != kNone && (prb[i] & kOwner)) {
+                const uint32_t rb = prb[i] & 0xFFFFu;
+                const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
                 int dy, dx;
                 first_px(M[rb], dy, dx);
                 const int y = 2 * int(rb / TBW) + dy, x = 2 * int(rb % TBW) + dx;
-                uint32_t rank = __popc(RB[y][x >> 5] & ((1u << (x & 31)) - 1u));
-                for (int k = 0; k < (x >> 5); ++k) rank += __popc(RB[y][k]);
                 const int64_t node = t * MAXB + j;
                 w.nroot[node] = uint16_t(rb);
                 w.nkey[node] = uint32_t(int64_t(y0 + y) * im.cols + (x0 + x));
-                w.nlrank[node] = uint16_t(rank);
                 w.gp[node] = uint32_t(node);
             }
             w.perim[t * NPERIM + p] = ent;
@@ -474,14 +516,20 @@ __global__ void __launch_bounds__(K1_NT, 6) k_tile_local_2d(ImgList2D L, Work w)
 // ---------------------------------------------------------------------------------------------
 namespace {
 
+// A root linked under another leaves its segment's root count and the root bitmap of its tile
+// (so that after the merge the bitmaps hold exactly the components' first pixels).
 __device__ __forceinline__ void link_dec(const Img2D &im, Work &w, uint32_t key)
 {
     const int64_t y = key / uint32_t(im.cols), x = key - y * im.cols;
-    dec_u8(w.segcnt, im.seg_base + y * im.tiles_x + x / TW);
+    const int64_t ty = y / TH, tx = x / TW;
+    dec_u8(w.segcnt, im.seg_base + y * im.tiles_x + tx);
+    const int ly = int(y - ty * TH), lx = int(x - tx * TW);
+    atomicAnd(w.rbits + (im.tile_base + ty * im.tiles_x + tx) * (TH * (TW / 32)) + ly * (TW / 32) + (lx >> 5),
+              ~(1u << (lx & 31)));
 }
 
 // Union of two nodes of one image; the root with the larger key is linked under the other, and
-// the linked root leaves its segment's root count.
+// the linked root leaves its segment's root count and its tile's root bitmap.
 __device__ void gunion2d(const Img2D &im, Work &w, uint32_t a, uint32_t b)
 {
     gunion_keyed(w.gp, w.nkey, a, b, [&](uint32_t key) { link_dec(im, w, key); });
@@ -627,48 +675,38 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Post-merge ranks of the surviving border roots (one CTA per tile).
+// Segment scan and node flatten, one launch: items below n_chunks scan a chunk of segment counts
+// (single pass, look-back); the others point every linked node of one tile straight at its global
+// root (all unions are done, so every writer stores the same final root), so that the label
+// writes find each root in one step however long the merge's chains grew.
 // ---------------------------------------------------------------------------------------------
-__device__ void post_tile_2d(const ImgList2D &L, Work &w, int64_t t)
+__global__ void __launch_bounds__(kScanThreads) k_scan_flatten_2d(Work w)
 {
-    __shared__ uint32_t LB[TH][TW / 32];   // first pixels of the tile's linked nodes
-    const Img2D im = L.get(t);
-    const int64_t lt = t - im.tile_base;
-    const int ty = int(lt / im.tiles_x), tx = int(lt - int64_t(ty) * im.tiles_x);
-    const int y0 = ty * TH, x0 = tx * TW;
-    const uint32_t nb = w.nb[t];
-    for (int i = threadIdx.x; i < TH * (TW / 32); i += blockDim.x) (&LB[0][0])[i] = 0;
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
-        const int64_t node = t * MAXB + j;
-        if (w.gp[node] == uint32_t(node)) continue;
-        // All unions are done: point the node's whole path at its root, so that the label pass
-        // (and the other tiles' walks here) find it in one step.
-        {
-            const uint32_t root = gfind_ro(w.gp, uint32_t(node));
-            for (uint32_t y = uint32_t(node); y != root;) {
+    grid_dep_wait();
+    grid_dep_release();   // after the wait: the label-write launch relies on it
+    __shared__ uint32_t tmp[kScanThreads / 32 + 1];
+    __shared__ uint32_t sh[2];
+    __shared__ uint32_t qslot;
+    const int64_t n = int64_t(w.n_chunks) + w.n_tiles;
+    ItemLoop loop{w.queue ? w.queue + 2 : nullptr, n};
+    for (int64_t it = loop.first(&qslot); it < n; it = loop.next(it, &qslot)) {
+        if (it < w.n_chunks) {
+            segscan_lb_chunk<kScanThreads>(w, tmp, sh);
+            continue;
+        }
+        const int64_t t = it - w.n_chunks;
+        const uint32_t nb = w.nb[t];
+        for (uint32_t j = threadIdx.x; j < nb; j += kScanThreads) {
+            const uint32_t node = uint32_t(t * MAXB + j);
+            if (w.gp[node] == node) continue;
+            const uint32_t root = gfind_ro(w.gp, node);
+            for (uint32_t y = node; y != root;) {
                 const uint32_t ny = w.gp[y];
                 w.gp[y] = root;
                 y = ny;
             }
         }
-        const uint32_t k = w.nkey[node];
-        const uint32_t y = k / uint32_t(im.cols);
-        const int ly = int(y) - y0, lx = int(k - y * uint32_t(im.cols)) - x0;
-        atomicOr(&LB[ly][lx >> 5], 1u << (lx & 31));
     }
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
-        const int64_t node = t * MAXB + j;
-        if (w.gp[node] != uint32_t(node)) continue;
-        const uint32_t k = w.nkey[node];
-        const uint32_t y = k / uint32_t(im.cols);
-        const int ly = int(y) - y0, lx = int(k - y * uint32_t(im.cols)) - x0;
-        uint32_t cnt = __popc(LB[ly][lx >> 5] & ((1u << (lx & 31)) - 1u));
-        for (int q = 0; q < (lx >> 5); ++q) cnt += __popc(LB[ly][q]);
-        w.grank[node] = w.nlrank[node] - cnt;
-    }
-    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -678,9 +716,8 @@ constexpr int K3_NT = 256;
 constexpr int RBWORDS = TH * (TW / 32);   // root-bitmap words per tile
 constexpr int RW = TW / 32;               // root-bitmap words per pixel row
 
-__global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
+__global__ void __launch_bounds__(K3_NT, 8) k_tile_write_2d(ImgList2D L, Work w)
 {
-    grid_dep_wait();
     __shared__ __align__(16) uint16_t Ls[NBLK];
     __shared__ uint32_t LT[NBLK];
     __shared__ uint32_t RB[RBWORDS];
@@ -696,28 +733,21 @@ __global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
         const int ty = int(lt / im.tiles_x), tx = int(lt - int64_t(ty) * im.tiles_x);
         const int y0 = ty * TH, x0 = tx * TW;
         const int nrp = min(TH, im.rows - y0), ncp = min(TW, im.cols - x0);
-        const uint32_t base0 = w.segpref[im.seg_base];
-
+        // Block entries and the root bitmap (first pixels of the components that stayed roots
+        // through the merge) were final before this grid's predecessor (segment scan and node
+        // flatten) started: that grid waits for the merge to complete before it lets this one launch.  So they are
+        // read before the wait (through L2), and only the segment prefixes, which the scan writes,
+        // after it.
         for (int i = tid; i < NBLK / 8; i += K3_NT)
-            reinterpret_cast<uint4 *>(Ls)[i] = reinterpret_cast<const uint4 *>(lab + t * NBLK)[i];
-        for (int i = tid; i < RBWORDS; i += K3_NT) RB[i] = w.rbits[t * RBWORDS + i];
+            reinterpret_cast<uint4 *>(Ls)[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + i);
+        for (int i = tid; i < RBWORDS; i += K3_NT) RB[i] = __ldcg(w.rbits + t * RBWORDS + i);
+        const uint32_t nb = __ldcg(w.nb + t);
+        grid_dep_wait();   // segment prefixes from here on (returns at once after the first tile)
+        const uint32_t base0 = w.segpref[im.seg_base];
         if (tid < TH && tid < nrp)
             segb[tid] = w.segpref[im.seg_base + int64_t(y0 + tid) * im.tiles_x + tx] - base0;
         if (lt == 0 && tid == 0)
             w.ncomp[im.index] = int64_t(w.segpref[im.seg_base + int64_t(im.rows) * im.tiles_x] - base0);
-        __syncthreads();
-
-        // Border roots linked under another tile's root are not roots any more.
-        const uint32_t nb = w.nb[t];
-        for (uint32_t j = tid; j < nb; j += K3_NT) {
-            const int64_t node = t * MAXB + j;
-            if (w.gp[node] == uint32_t(node)) continue;
-            const uint32_t rb = w.nroot[node];
-            int dy, dx;
-            first_px(Ls[rb] >> 12, dy, dx);
-            const int y = 2 * int(rb / TBW) + dy, x = 2 * int(rb % TBW) + dx;
-            atomicAnd(&RB[y * (TW / 32) + (x >> 5)], ~(1u << (x & 31)));
-        }
         __syncthreads();
 
         // Surviving roots: rank = roots before it in its row segment.  RW consecutive lanes hold
@@ -741,14 +771,21 @@ __global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
                 bits &= bits - 1;
             }
         }
+        // Border components linked under another tile's component: the label of that root, its
+        // segment's prefix plus its rank among the first pixels left in its row of its tile.
         for (uint32_t j = tid; j < nb; j += K3_NT) {
             const int64_t node = t * MAXB + j;
-            if (w.gp[node] == uint32_t(node)) continue;
-            const uint32_t g = gfind_ro(w.gp, uint32_t(node));
-            const uint32_t kg = w.nkey[g];
+            if (__ldcg(w.gp + node) == uint32_t(node)) continue;
+            const uint32_t g = gfind_halve(w.gp, uint32_t(node));
+            const uint32_t kg = __ldcg(w.nkey + g);
             const int64_t yg = kg / uint32_t(im.cols), xg = kg - yg * im.cols;
-            const uint32_t sb = w.segpref[im.seg_base + yg * im.tiles_x + xg / TW] - base0;
-            LT[w.nroot[node]] = 1u + sb + w.grank[g];
+            const int64_t tyg = yg / TH, txg = xg / TW;
+            const int ly = int(yg - tyg * TH), lx = int(xg - txg * TW);
+            const uint32_t *rw = w.rbits + (im.tile_base + tyg * im.tiles_x + txg) * RBWORDS + ly * RW;
+            uint32_t rank = __popc(__ldcg(rw + (lx >> 5)) & ((1u << (lx & 31)) - 1u));
+            for (int k = 0; k < (lx >> 5); ++k) rank += __popc(__ldcg(rw + k));
+            const uint32_t sb = w.segpref[im.seg_base + yg * im.tiles_x + txg] - base0;
+            LT[__ldcg(w.nroot + node)] = 1u + sb + rank;
         }
         __syncthreads();
 
@@ -786,24 +823,6 @@ __global__ void __launch_bounds__(K3_NT) k_tile_write_2d(ImgList2D L, Work w)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Post-merge pass: border-root ranks (items < n_tiles) and scan-chunk sums (the rest).
-// ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPostThreads) k_post_2d(ImgList2D L, Work w)
-{
-    grid_dep_wait();
-    grid_dep_release();
-    __shared__ uint32_t tmp[kPostThreads / 32 + 1];
-    __shared__ uint32_t qslot;
-    const int64_t n = w.n_tiles + w.n_chunks;
-    ItemLoop loop{w.queue ? w.queue + 2 : nullptr, n};
-    for (int64_t it = loop.first(&qslot); it < n; it = loop.next(it, &qslot)) {
-        if (it < w.n_tiles) post_tile_2d(L, w, it);
-        else chunk_sum<kPostThreads>(w, it - w.n_tiles, tmp);
-    }
-}
-
-
-// ---------------------------------------------------------------------------------------------
 // Geometry and launch sequence of this tile shape.
 // ---------------------------------------------------------------------------------------------
 inline Geometry geometry()
@@ -836,16 +855,14 @@ inline cudaError_t launch(const ImgList2D &L, const Work &w, int sms, bool persi
         if (e == cudaSuccess) e = r;
     };
     mark(0);
-    k_tile_local_2d<<<grid(w.n_tiles, 6), K1_NT, 0, s>>>(L, wk);
+    k_tile_local_2d<<<grid(w.n_tiles, 7), K1_NT, 0, s>>>(L, wk);
     keep(cudaGetLastError());
     mark(1);
     keep(launch_k(k_merge_2d, grid(w.n_tiles, 8), K2_NT, s, ov, L, wk));
     mark(2);
-    keep(launch_k(k_post_2d, grid(w.n_tiles + w.n_chunks, 12), kPostThreads, s, ov, L, wk));
+    keep(launch_k(k_scan_flatten_2d, grid(int64_t(w.n_chunks) + w.n_tiles, 8), kScanThreads, s, ov, wk));
     mark(3);
-    keep(launch_k(k_segscan, unsigned(std::max(w.n_chunks, 1)), kScanThreads, s, ov, wk));
+    keep(launch_k(k_tile_write_2d, grid(w.n_tiles, 8), K3_NT, s, ov, L, wk));
     mark(4);
-    keep(launch_k(k_tile_write_2d, grid(w.n_tiles, 6), K3_NT, s, ov, L, wk));
-    mark(5);
     return e;
 }

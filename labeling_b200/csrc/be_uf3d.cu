@@ -137,7 +137,7 @@ __device__ __forceinline__ bool perim_pos3(int p, const TileGeo &g, int &f, int 
 namespace {
 
 constexpr int NT1 = kT3LocalThreads;   // threads of the tile-local kernel: one per block row
-constexpr int MQ1 = 2048;          // merge-queue capacity per round (more are merged in place)
+constexpr int MQ1 = 1536;          // union-queue capacity (more are merged in place)
 static_assert(TB2 == 32, "a block row along d2 is one 32-bit word");
 static_assert(NBLK <= 4096, "run starts must fit 12 bits");
 
@@ -170,14 +170,19 @@ __device__ __forceinline__ uint32_t slot_block(uint32_t slot)
     return (b0 * TB1 + b1) * TB2 + b2;
 }
 
+// Shared-memory position of block x's union-find entry: the low five bits (the block's place along
+// d2) are XOR-ed with its row, so that the 32 lanes of a warp -- 32 rows walking the same position
+// -- reach 32 different banks.  Entries still name blocks by their plain index.
+__device__ __forceinline__ uint32_t sw3(uint32_t x) { return x ^ ((x >> 5) & 31u); }
+
 // Union-find over run starts, the slot carried in the entry: (slot << 12) | parent.
 __device__ __forceinline__ uint32_t efind3(uint32_t *P, uint32_t x)
 {
-    uint32_t v = P[x];
+    uint32_t v = P[sw3(x)];
     while ((v & 0xFFFu) != x) {
         const uint32_t y = v & 0xFFFu;
-        const uint32_t vg = P[y];
-        if ((vg & 0xFFFu) != y) P[x] = vg;
+        const uint32_t vg = P[sw3(y)];
+        if ((vg & 0xFFFu) != y) P[sw3(x)] = vg;
         x = y;
         v = vg;
     }
@@ -186,10 +191,10 @@ __device__ __forceinline__ uint32_t efind3(uint32_t *P, uint32_t x)
 
 __device__ __forceinline__ uint32_t efind3_ro(const uint32_t *P, uint32_t x)
 {
-    uint32_t v = P[x];
+    uint32_t v = P[sw3(x)];
     while ((v & 0xFFFu) != x) {
         x = v & 0xFFFu;
-        v = P[x];
+        v = P[sw3(x)];
     }
     return x;
 }
@@ -197,11 +202,11 @@ __device__ __forceinline__ uint32_t efind3_ro(const uint32_t *P, uint32_t x)
 // As efind3, also returning the root's own entry as read (the union compares the two).
 __device__ __forceinline__ uint32_t efind3_e(uint32_t *P, uint32_t x, uint32_t &ev)
 {
-    uint32_t v = P[x];
+    uint32_t v = P[sw3(x)];
     while ((v & 0xFFFu) != x) {
         const uint32_t y = v & 0xFFFu;
-        const uint32_t vg = P[y];
-        if ((vg & 0xFFFu) != y) P[x] = vg;
+        const uint32_t vg = P[sw3(y)];
+        if ((vg & 0xFFFu) != y) P[sw3(x)] = vg;
         x = y;
         v = vg;
     }
@@ -217,11 +222,11 @@ __device__ __forceinline__ void eunion3(uint32_t *P, uint32_t a, uint32_t b)
         b = efind3_e(P, b, eb);
         if (a == b) return;
         if (ea < eb) {
-            const uint32_t old = atomicMin(&P[b], ea);
+            const uint32_t old = atomicMin(&P[sw3(b)], ea);
             if ((old & 0xFFFu) == b) return;
             b = old & 0xFFFu;
         } else {
-            const uint32_t old = atomicMin(&P[a], eb);
+            const uint32_t old = atomicMin(&P[sw3(a)], eb);
             if ((old & 0xFFFu) == a) return;
             a = old & 0xFFFu;
         }
@@ -250,7 +255,7 @@ __device__ __forceinline__ void split16b(uint4 v, uint32_t K, bool hi, uint32_t 
 
 }  // namespace
 
-__global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
+__global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
 {
     grid_dep_release();   // the merge launch may take free SMs during this grid's last wave
     __shared__ uint32_t P[NBLK];               // run starts: (slot << 12) | parent
@@ -260,8 +265,8 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
     __shared__ uint32_t RB[TX * TY * RBW];
     __shared__ uint32_t BF[NBLK / 32];
     __shared__ uint32_t BP[NBLK / 32];
-    __shared__ uint32_t MQ[MQ1];               // merge queue: (start_a << 16) | start_b
-    __shared__ uint32_t mqn[4];
+    __shared__ uint32_t MQ[MQ1];               // union queue: (block_a << 16) | block_b
+    __shared__ uint32_t mqn[4];                // queue counts of the union rounds
     __shared__ uint32_t tmp[NT1 / 32 + 1];
     __shared__ uint32_t qslot;
 
@@ -354,7 +359,7 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
                 else if (H10 & span) { i = 1; j = 0; m = H10 & span; }
                 else { i = 1; j = 1; m = H11 & span; }
                 const uint32_t x = rowb + s0;
-                P[x] = (slot3(b0, i, b1, j, __ffs(m) - 1) << 12) | x;
+                P[sw3(x)] = (slot3(b0, i, b1, j, __ffs(m) - 1) << 12) | x;
             }
         }
         __syncthreads();
@@ -362,7 +367,9 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
         // Phase B: links to the four preceding rows (d0-1 with d1-1 / d1 / d1+1, and d0 with
         // d1-1), each with offsets dz = -1 / 0 / +1 along d2.  As in 2D, a link is dropped when
         // an earlier one (further along d2, or dz = 0 before dz = +-1 at the same block) joins the
-        // same two runs.  One round per neighbour row: queue, then merge with every lane.
+        // same two runs.
+        uint32_t LN[4], LW[4], LE[4];
+        int UR[4];
 #pragma unroll
         for (int nr = 0; nr < 4; ++nr) {
             const int dx = nr < 3 ? -1 : 0, dy = nr < 3 ? nr - 1 : -1;
@@ -395,79 +402,119 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
                 NW = nw & ~((n0 & uhl) | (hl & Nsh));
                 NE = ne & ~((n0 & uhz) | (hl & NEsh & uhz));
             }
-            const uint32_t n = __popc(N) + __popc(NW) + __popc(NE);
-            uint32_t pos = warp_reserve(&mqn[nr], n);
-            // The queue holds the two blocks of each link; their run starts are looked up by the
-            // merging lanes, which share that work evenly.
-            auto start_of = [&](uint32_t b) -> uint32_t {
-                return (b & ~31u) + hibit3(WS[b >> 5] & ((2u << (b & 31u)) - 1u));
+            LN[nr] = N;
+            LW[nr] = NW;
+            LE[nr] = NE;
+            UR[nr] = ur;
+        }
+        auto start_of = [&](uint32_t b) -> uint32_t {
+            return (b & ~31u) + hibit3(WS[b >> 5] & ((2u << (b & 31u)) - 1u));
+        };
+        // Forest: a run takes its first link into the preceding layer (d0 - 1, whose slots are all
+        // smaller than this row's) as its parent, by a plain store of the parent's entry (its own
+        // root entry, or already its own parent's: an ancestor either way).  These links leave the
+        // queue.  Links within the same layer (d1 - 1) may go to larger slots and stay unions.
+        // (Pointer jumping over the forest before the unions was measured slower.)
+        {
+            uint32_t ss = S;
+            while (ss) {
+                const uint32_t s0 = __ffs(ss) - 1;
+                ss &= ss - 1;
+                const uint32_t brk = ~hz & (~0u << s0);
+                const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
+                const uint32_t span = (~0u << s0) & (0xFFFFFFFFu >> (31u - e));
+                bool found = false;
+#pragma unroll
+                for (int nr = 0; nr < 3; ++nr) {
+                    const uint32_t lk = (LN[nr] | LW[nr] | LE[nr]) & span;
+                    if (found || !lk) continue;
+                    found = true;
+                    const uint32_t k = __ffs(lk) - 1, bit = 1u << k;
+                    const uint32_t ubase = uint32_t(UR[nr]) * TB2;
+                    uint32_t tgt;
+                    if (LN[nr] & bit) {
+                        tgt = ubase + k;
+                        LN[nr] &= ~bit;
+                    } else if (LW[nr] & bit) {
+                        tgt = ubase + k - 1;
+                        LW[nr] &= ~bit;
+                    } else {
+                        tgt = ubase + k + 1;
+                        LE[nr] &= ~bit;
+                    }
+                    P[sw3(rowb + s0)] = P[sw3(start_of(tgt))];
+                }
+            }
+        }
+        __syncthreads();
+        // The remaining links are unions, queued and merged by every lane, one neighbour row per
+        // round (the queue then holds a round's links; fewer rounds overflowed it and left the
+        // overflow to the warps that queued last).
+#pragma unroll
+        for (int round = 0; round < 4; ++round) {
+            const int nr0 = round, nr1 = round + 1;
+            uint32_t n = 0;
+#pragma unroll
+            for (int nr = 0; nr < 4; ++nr)
+                if (nr >= nr0 && nr < nr1) n += __popc(LN[nr]) + __popc(LW[nr]) + __popc(LE[nr]);
+            uint32_t pos = warp_reserve(&mqn[round], n);
+            auto push = [&](uint32_t a, uint32_t b) {
+                if (pos < uint32_t(MQ1)) MQ[pos] = (a << 16) | b;
+                else eunion3(P, start_of(a), start_of(b));   // queue full: merge in place
+                ++pos;
             };
-            {
-                const uint32_t ubase = uint32_t(ur) * TB2;
-                auto push = [&](uint32_t a, uint32_t b) {
-                    if (pos < uint32_t(MQ1)) MQ[pos] = (a << 16) | b;
-                    else eunion3(P, start_of(a), start_of(b));   // queue full: merge in place
-                    ++pos;
-                };
-                uint32_t todo = N | NW | NE;
+#pragma unroll
+            for (int nr = 0; nr < 4; ++nr) {
+                if (nr < nr0 || nr >= nr1) continue;
+                const uint32_t ubase = uint32_t(UR[nr]) * TB2;
+                uint32_t todo = LN[nr] | LW[nr] | LE[nr];
                 while (todo) {
                     const uint32_t k = __ffs(todo) - 1;
                     todo &= todo - 1;
                     const uint32_t bit = 1u << k;
                     const uint32_t a = rowb + k;
-                    if (N & bit) push(a, ubase + k);
-                    if (NW & bit) push(a, ubase + k - 1);
-                    if (NE & bit) push(a, ubase + k + 1);
+                    if (LN[nr] & bit) push(a, ubase + k);
+                    if (LW[nr] & bit) push(a, ubase + k - 1);
+                    if (LE[nr] & bit) push(a, ubase + k + 1);
                 }
             }
             __syncthreads();
-            const uint32_t nq = min(mqn[nr], uint32_t(MQ1));
+            const uint32_t nq = min(mqn[round], uint32_t(MQ1));
             // Contiguous runs of the queue per thread, as in 2D.
             const uint32_t per = (nq + NT1 - 1) / NT1, lo = min(nq, uint32_t(tid) * per), hi = min(nq, lo + per);
             for (uint32_t q = lo; q < hi; ++q) eunion3(P, start_of(MQ[q] >> 16), start_of(MQ[q] & 0xFFFFu));
             __syncthreads();
         }
 
-        // Phase C: every run start points straight at its root; roots mark their first voxel.
-        // The starts are listed (16-bit, in the free merge queue) and taken round robin, so the
-        // work is even over the lanes and a row's parents are mostly compressed already.
-        if (tid == 0) mqn[0] = 0;
-        __syncthreads();
-        uint16_t *runs = reinterpret_cast<uint16_t *>(MQ);
-        static_assert(2 * MQ1 >= NBLK, "the run list must hold every block");
+        // Phase C: every run start of this row, and every entry on its path, points straight at its
+        // root (a read-only walk, then the root's entry stored along the path: every writer stores
+        // the same final entry); roots mark their first voxel.
         {
-            uint32_t pos = warp_reserve(&mqn[0], __popc(S));
             uint32_t ss = S;
             while (ss) {
-                const uint32_t s0 = __ffs(ss) - 1;
+                const uint32_t x = rowb + (__ffs(ss) - 1);
                 ss &= ss - 1;
-                runs[pos++] = uint16_t(rowb + s0);
-            }
-        }
-        __syncthreads();
-        {
-            const uint32_t nruns = mqn[0];
-            for (uint32_t i = tid; i < nruns; i += NT1) {
-                const uint32_t x = runs[i];
-                const uint32_t root = efind3_ro(P, x);
-                const uint32_t ev = P[root];
-                for (uint32_t y = x; y != root;) {
-                    const uint32_t ny = P[y] & 0xFFFu;
-                    P[y] = ev;
+                uint32_t root = x, ev = P[sw3(x)];
+                for (int it = 0; (ev & 0xFFFu) != root && it < NBLK; ++it) {   // acyclic: the cap never binds
+                    root = ev & 0xFFFu;
+                    ev = P[sw3(root)];
+                }
+                for (uint32_t y = x, it = 0; y != root && it < NBLK; ++it) {
+                    const uint32_t ny = P[sw3(y)] & 0xFFFu;
+                    P[sw3(y)] = ev;
                     y = ny;
                 }
-                if (root == x) {
-                    const uint32_t rb = slot_block(ev >> 12);
-                    const uint32_t key = local_key(int(rb), M[rb]);
-                    const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
-                    if (GUARD(w, key < uint32_t(TX * TY * TZ), 101, key))
-                        atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
-                }
+                if (root != x) continue;
+                const uint32_t rb = slot_block(ev >> 12);
+                const uint32_t key = local_key(int(rb), M[rb]);
+                const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
+                if (GUARD(w, key < uint32_t(TX * TY * TZ), 101, key))
+                    atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
             }
         }
-        __syncthreads();
         // Block entries: the root block of a component carries ROOT_FLAG | its first-voxel key,
-        // every other block its root block.
+        // every other block its root block.  (Runs do not cross rows: every start read here is
+        // this thread's own.)
         {
             uint32_t cur = 0;
 #pragma unroll
@@ -477,7 +524,7 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int k = 4 * h + q;
-                    if ((S >> k) & 1u) cur = slot_block(P[rowb + k] >> 12);
+                    if ((S >> k) & 1u) cur = slot_block(P[sw3(rowb + k)] >> 12);
                     const uint32_t m = (mm >> (8 * q)) & 0xFFu;
                     uint32_t v = 0;
                     if (m) {
@@ -489,6 +536,7 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
                 reinterpret_cast<uint4 *>(lab + t * NBLK + rowb)[h] = make_uint4(e[0], e[1], e[2], e[3]);
             }
         }
+        __syncthreads();   // root bitmap complete; every run start points at its root
 
         // Phase D: segment counts and border nodes.
         for (int r = tid; r < TX * TY; r += NT1) {
@@ -503,7 +551,7 @@ __global__ void __launch_bounds__(NT1, 5) k_tile_local_3d(ImgList3D L, Work w)
         auto root_block = [&](int b) -> uint32_t {
             const uint32_t row = uint32_t(b) >> 5, k = uint32_t(b) & 31u;
             const uint32_t st = hibit3(WS[row] & ((2u << k) - 1u));
-            return slot_block(P[(row << 5) + st] >> 12);
+            return slot_block(P[sw3((row << 5) + st)] >> 12);
         };
         for (int p = tid; p < NPERIM; p += NT1) {
             int f, pb0, pb1, pb2;
@@ -890,7 +938,6 @@ __global__ void __launch_bounds__(kPostThreads) k_post_3d(ImgList3D L, Work w)
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
 {
-    grid_dep_wait();
     __shared__ __align__(16) uint32_t Ls[NBLK];
     __shared__ uint32_t LT[NBLK];
     __shared__ uint32_t RB[TX * TY * RBW];
@@ -903,19 +950,15 @@ __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
     for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
         const Img3D im = L.get(t);
         const TileGeo g = tile_geo(im, t);
-        const uint32_t base0 = w.segpref[im.seg_base];
         const int64_t rs0 = int64_t(im.d1) * im.d2;
 
+        // Block entries and the post-merge node state were final before this grid's predecessor
+        // (the segment scan) started: that grid waits for the post-merge pass to complete before it
+        // lets this one launch.  So the root bitmap is built before the wait (reads through L2);
+        // only the segment prefixes, which the scan writes, come after it.
         for (int i = tid; i < NBLK / 4; i += NT)
-            reinterpret_cast<uint4 *>(Ls)[i] = reinterpret_cast<const uint4 *>(lab + t * NBLK)[i];
+            reinterpret_cast<uint4 *>(Ls)[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + i);
         for (int i = tid; i < TX * TY * RBW; i += NT) RB[i] = 0;
-        for (int r = tid; r < TX * TY; r += NT) {
-            const int X = r / TY, Y = r % TY;
-            if (X < g.nx && Y < g.ny)
-                segb[r] = w.segpref[im.seg_base + (int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.t2 + g.tx2] - base0;
-        }
-        if (t == im.tile_base && tid == 0)
-            w.ncomp[im.index] = int64_t(w.segpref[im.seg_base + int64_t(im.d0) * im.d1 * im.t2] - base0);
         __syncthreads();
 
         for (int b = tid; b < NBLK; b += NT) {
@@ -927,15 +970,25 @@ __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
                 atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
         }
         __syncthreads();
-        const uint32_t nb = w.nb[t];
+        const uint32_t nb = __ldcg(w.nb + t);
         for (uint32_t j = tid; j < nb; j += NT) {
             const int64_t node = t * MAXB + j;
-            if (w.gp[node] == uint32_t(node)) continue;
-            if (!GUARD(w, w.nroot[node] < NBLK && (Ls[w.nroot[node] % NBLK] & ROOT_FLAG), 402, node)) continue;
-            const uint32_t key = Ls[w.nroot[node]] & (ROOT_FLAG - 1);
+            if (__ldcg(w.gp + node) == uint32_t(node)) continue;
+            const uint32_t nr = __ldcg(w.nroot + node);
+            if (!GUARD(w, nr < NBLK && (Ls[nr % NBLK] & ROOT_FLAG), 402, node)) continue;
+            const uint32_t key = Ls[nr] & (ROOT_FLAG - 1);
             const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
             atomicAnd(&RB[(X * TY + Y) * RBW + (Z >> 5)], ~(1u << (Z & 31)));
         }
+        grid_dep_wait();   // segment prefixes from here on (returns at once after the first tile)
+        const uint32_t base0 = w.segpref[im.seg_base];
+        for (int r = tid; r < TX * TY; r += NT) {
+            const int X = r / TY, Y = r % TY;
+            if (X < g.nx && Y < g.ny)
+                segb[r] = w.segpref[im.seg_base + (int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.t2 + g.tx2] - base0;
+        }
+        if (t == im.tile_base && tid == 0)
+            w.ncomp[im.index] = int64_t(w.segpref[im.seg_base + int64_t(im.d0) * im.d1 * im.t2] - base0);
         __syncthreads();
         for (int b = tid; b < NBLK; b += NT) {
             const uint32_t e = Ls[b];

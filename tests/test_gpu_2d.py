@@ -162,3 +162,31 @@ def test_run_equivalence_slot_matches_reference_kernels(ctx, golden):
         lab_alg.Label(img, coh=be.COH_4)
     with pytest.raises(ValueError):
         be.make_labeler("runeq", three_d=True)
+
+
+def test_iterative_graph_cache_reuse(ctx):
+    """The iterative and pixel forms keep their instantiated graph per size: a call with a new
+    image, new buffers or a new threshold at the same size reuses it (only the image arguments
+    change), a new size rebuilds it.  Every result exact, in both directions of the switch."""
+    import torch
+    import labeling_b200 as be
+    rng = np.random.default_rng(99)
+    for (h, w), thr in [((300, 400), 0), ((300, 400), 100), ((301, 400), 0), ((300, 400), 0), ((300, 400), 7)]:
+        img = rng.integers(0, 256, (h, w)).astype(np.uint8)
+        ref, k = O.ccl2d(img, thr)
+        lab, n = run2d(ctx, img, thr, algo=2)
+        assert n == k and np.array_equal(lab, ref), (h, w, thr)
+        lab, n = run2d(ctx, img, thr, algo=3)          # pixel form, 4-connected by default
+        ref4, k4 = O.ccl2d(img, thr, False)
+        assert n == k4 and np.array_equal(lab, ref4), (h, w, thr, "pixel 4")
+        d = torch.from_numpy(img).cuda()
+        out = torch.empty((h, w), dtype=torch.int32, device="cuda")
+        n8 = be.label2d(ctx, d, out, threshold=thr, algo=be.ALGO_PIXEL, coh=be.COH_8)
+        assert n8 == k and np.array_equal(out.cpu().numpy(), ref), (h, w, thr, "pixel")
+    for shape, thr in [((20, 30, 40), 0), ((20, 30, 40), 50), ((21, 30, 40), 0)]:
+        vol = rng.integers(0, 256, shape).astype(np.uint8)
+        ref, k = O.ccl3d(vol, thr)
+        d = torch.from_numpy(vol).cuda()
+        out = torch.empty(shape, dtype=torch.int32, device="cuda")
+        assert be.label3d(ctx, d, out, threshold=thr, algo=be.ALGO_ITER) == k
+        assert np.array_equal(out.cpu().numpy(), ref), (shape, thr)
