@@ -504,8 +504,8 @@ def bench_plain(args, rank, world, local_rank, workload):
                             "achieved_gbs": round(ab / (ms / 1e3) / 1e9, 1) if ab and ms else None})
         roofline["dominant_kernel"] = max(kernels, key=lambda k: k["ms"])["kernel"]
         roofline["stage_sum_ms"] = round(pipe_ms, 4)
-        # DRAM traffic of the launches from a committed ncu capture (profiles/traffic.json): a
-        # lower bound, since lines still dirty in L2 when a launch ends are written back later.
+        # DRAM bytes of the launches that have a committed ncu capture (profiles/traffic.json):
+        # a lower bound, since lines still dirty in L2 when a launch ends are written back later.
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         tr = None
         if os.path.exists(tp):
@@ -514,7 +514,6 @@ def bench_plain(args, rank, world, local_rank, workload):
             except Exception:
                 tr = None
         if tr:
-            roofline["traffic_ncu_lower_bound"] = int(tr["bytes_per_labeling"])
             for k in kernels:
                 k["ncu_dram_bytes"] = tr["per_kernel"].get(k["kernel"])
     clocks = clk.summary()

@@ -100,8 +100,14 @@ struct be_server {
     bool any = false;
     int64_t alloc_count = 0;
 
+    // Live free memory, read at most every kLiveRefresh (the query can stall the device queue);
+    // in between, the estimate follows the server's own admissions and releases.
+    size_t live_q = 0, used_q = 0;
+    Clock::time_point live_t{};
+    bool live_valid = false;
     void run();
     size_t live_headroom();
+    size_t live_estimate(bool refresh);
     bool launch(Lane &ln, std::vector<Req *> &batch);
     void finish(Lane &ln, int status);
     void *alloc(size_t bytes, cudaStream_t s, int *status);
@@ -138,6 +144,22 @@ size_t be_server::live_headroom()
         reserved = in_use = 0;
     }
     return fr + size_t(reserved > in_use ? reserved - in_use : 0);
+}
+
+size_t be_server::live_estimate(bool refresh)
+{
+    constexpr auto kLiveRefresh = std::chrono::milliseconds(20);
+    const Clock::time_point now = Clock::now();
+    if (refresh || !live_valid || now - live_t > kLiveRefresh) {
+        live_q = live_headroom();
+        used_q = used;
+        live_t = now;
+        live_valid = true;
+    }
+    // Memory the server admitted since the query is gone from the headroom; memory it released
+    // since is back (in its pool).
+    const size_t est = live_q + used_q;
+    return est > used ? est - used : 0;
 }
 
 // Copies in, labels and copies out one batch on lane `ln`; false when nothing could be started.
@@ -331,7 +353,8 @@ void be_server::run()
         bool started = false;
         if (free_lane && !pending.empty()) {
             std::vector<Req *> batch;
-            const size_t live = live_headroom();
+            size_t live = live_estimate(false);
+            bool refreshed = false;
             size_t take = 0;
             while (!pending.empty() && int(batch.size()) < cfg.max_batch) {
                 Req *q = pending.front();
@@ -352,6 +375,10 @@ void be_server::run()
                     continue;
                 }
                 if (used + need > budget) break;   // wait for memory to free up
+                if (take + need > live && !refreshed) {   // the estimate says no: read it again
+                    live = live_estimate(true);
+                    refreshed = true;
+                }
                 if (take + need > live) break;     // the device is fuller than the budget says
                 take += need;
                 pending.pop_front();
