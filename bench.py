@@ -264,7 +264,7 @@ def _time_cpu_alg(O, alg, images, budget_s):
     return px / t_total / 1e9, n, t_total
 
 
-def cpu_reference_2d(images, budget_s: float):
+def cpu_reference_2d(images, budget_s: float, main_alg: str = "bleq"):
     """Times the reference's CPU labelers (its main.cpp registry's CPU slots, compiled from its
     sources) on whole images, each by the reference's own stopwatch around DoLabel, all host
     threads for the OpenMP ones.  The block-equivalence labeler (the bleq CPU slot) is the
@@ -288,10 +288,10 @@ def cpu_reference_2d(images, budget_s: float):
         v, n, t = _time_cpu_alg(O, alg, images, budget_s / len(CPU_ALGS_2D))
         res[alg] = {"value": round(v, 4), "cores": 1 if alg == "gr-block" else cores,
                     "sample": f"{n} whole images, {t:.2f} s", "what": CPU_ALGS_2D[alg]}
-    main = res["bleq"]
-    return {"value": main["value"], "unit": "Gpx/s", "cores": cores, "kind": "reference",
-            "sample": f"bleq CPU slot ({CPU_ALGS_2D['bleq']}), {main['sample']}, reference stopwatch",
-            "others": {k: v for k, v in res.items() if k != "bleq"}, **host_info()}
+    main = res[main_alg]
+    return {"value": main["value"], "unit": "Gpx/s", "cores": main["cores"], "kind": "reference",
+            "sample": f"{main_alg} CPU slot ({CPU_ALGS_2D[main_alg]}), {main['sample']}, reference stopwatch",
+            "others": {k: v for k, v in res.items() if k != main_alg}, **host_info()}
 
 
 def cpu_reference_3d(volumes, budget_s: float):
@@ -321,7 +321,7 @@ def cpu_reference_3d(volumes, budget_s: float):
             **host_info()}
 
 
-def check_against_oracle(items, threads: int = 8) -> dict:
+def check_against_oracle(items, threads: int = 8, conn8: bool = True) -> dict:
     """Parity of timed label maps, part of the cpu_baseline leg (outside every timed region):
     items are (name, image, labels as numpy, count); each is compared with the oracle's canonical
     labels (oracle/be_oracle.c, union-find restatement) in a thread pool.  Returns the number of
@@ -331,7 +331,7 @@ def check_against_oracle(items, threads: int = 8) -> dict:
 
     def one(it):
         name, img, lab, n = it
-        ref, k = O.ccl2d(img) if img.ndim == 2 else O.ccl3d(img)
+        ref, k = O.ccl2d(img, 0, conn8) if img.ndim == 2 else O.ccl3d(img)
         d = int(np.count_nonzero(lab != ref))
         return name, d, int(n) != int(k)
 
@@ -342,7 +342,7 @@ def check_against_oracle(items, threads: int = 8) -> dict:
             "images_checked": len(res),
             "count_mismatches": [nm for nm, _, c in res if c],
             "mismatched_images": [nm for nm, d, _ in res if d],
-            "checker": "oracle (CPU union-find restatement), every timed image once",
+            "checker": f"oracle (CPU union-find restatement, {'8' if conn8 else '4'}-connectivity in 2D), every timed image once",
             "check_s": round(time.perf_counter() - t0, 2)}
 
 
@@ -357,8 +357,10 @@ def bench_plain(args, rank, world, local_rank, workload):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     is3d = workload == "3d512"
-    algo = be.ALGO_ITER if args.algo == "iter" else be.ALGO_UF
-    form = "iterative scan/analyze" if args.algo == "iter" else "union-find"
+    algo = {"uf": be.ALGO_UF, "iter": be.ALGO_ITER, "runs": be.ALGO_RUNS}[args.algo]
+    form = {"uf": "union-find", "iter": "iterative scan/analyze", "runs": "run equivalence (4-connected)"}[args.algo]
+    if is3d and algo == be.ALGO_RUNS:
+        raise SystemExit("run equivalence is 2D only")
     if is3d:
         inputs = make_3d_inputs(512, seed=replicas.replica_seed(100, rank),
                                 only=args.families if args.workload == "3d512" else "")
@@ -375,6 +377,8 @@ def bench_plain(args, rank, world, local_rank, workload):
         metric, unit = f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "Gpx/s"
     if algo == be.ALGO_ITER:
         metric = metric.replace("BE,", "BE iterative,")
+    if algo == be.ALGO_RUNS:
+        metric = metric.replace("BE, 8-conn", "run equivalence, 4-conn")
 
     ctx = be.Context(local_rank)
     stream = torch.cuda.Stream(device=dev)
@@ -386,7 +390,8 @@ def bench_plain(args, rank, world, local_rank, workload):
     def label(i, want=False):
         if is3d:
             return be.label3d(ctx, d_in[i], d_out[i], want_count=want, stream=stream, algo=algo)
-        return be.label2d(ctx, d_in[i], d_out[i], want_count=want, stream=stream, algo=algo)
+        coh = be.COH_4 if algo == be.ALGO_RUNS else be.COH_DEFAULT
+        return be.label2d(ctx, d_in[i], d_out[i], want_count=want, stream=stream, algo=algo, coh=coh)
 
     with torch.cuda.stream(stream):
         for i in range(max(args.warmup, 3)):
@@ -442,15 +447,16 @@ def bench_plain(args, rank, world, local_rank, workload):
     h_in = [torch.from_numpy(a).pin_memory() for _, a in inputs]
     h_out = [torch.empty(a.shape, dtype=torch.int32).pin_memory() for _, a in inputs]
     host_call = be.label3d_host if is3d else be.label2d_host
+    host_kw = {"coh": be.COH_4} if algo == be.ALGO_RUNS else {}
     for i in range(min(2, len(inputs))):
-        host_call(ctx, h_in[i].numpy(), out=h_out[i].numpy(), algo=algo)
+        host_call(ctx, h_in[i].numpy(), out=h_out[i].numpy(), algo=algo, **host_kw)
     t0 = time.perf_counter()
     e2e_px = 0
     e2e_steps = max(1, min(args.steps, 2 * len(inputs)))
     h2d = d2h = 0
     for s in range(e2e_steps):
         i = s % len(inputs)
-        host_call(ctx, h_in[i].numpy(), out=h_out[i].numpy(), algo=algo)
+        host_call(ctx, h_in[i].numpy(), out=h_out[i].numpy(), algo=algo, **host_kw)
         e2e_px += npx[i]
         h2d += npx[i]
         d2h += 4 * npx[i] + 8
@@ -533,9 +539,12 @@ def bench_plain(args, rank, world, local_rank, workload):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         budget = 20.0
-        result["cpu_baseline"] = (cpu_reference_3d if is3d else cpu_reference_2d)(inputs, budget)
+        if is3d:
+            result["cpu_baseline"] = cpu_reference_3d(inputs, budget)
+        else:
+            result["cpu_baseline"] = cpu_reference_2d(inputs, budget, "runeq" if algo == be.ALGO_RUNS else "bleq")
         items = [(n, a, o.cpu().numpy(), c) for (n, a), o, c in zip(inputs, d_out, counts)]
-        result["parity"] = check_against_oracle(items)
+        result["parity"] = check_against_oracle(items, conn8=algo != be.ALGO_RUNS)
         result["mismatched_labels"] = result["parity"]["mismatched_labels"]
     ctx.close()
     return result
@@ -828,13 +837,15 @@ def bench_reference(args, rank, world):
             if args.families and args.workload == workload:
                 names = args.families.split(",")
             inputs = make_2d_inputs(side, names, seed=10)
-            cb = cpu_reference_2d(inputs, budget_s=budget)
+            cb = cpu_reference_2d(inputs, budget_s=budget, main_alg="runeq" if args.algo == "runs" else "bleq")
             metric, unit = f"Gpx/s labeled (2D {side}^2 BE, 8-conn)", "Gpx/s"
         if cb is None:
             return None
-        form = "iterative scan/analyze" if args.algo == "iter" else "union-find"
+        form = {"uf": "union-find", "iter": "iterative scan/analyze", "runs": "run equivalence (4-connected)"}[args.algo]
         if args.algo == "iter":
             metric = metric.replace("BE,", "BE iterative,")
+        if args.algo == "runs":
+            metric = metric.replace("BE, 8-conn", "run equivalence, 4-conn")
         return {"impl": "reference", "metric": metric, "value": round(cb["value"], 4),
                 "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
@@ -850,7 +861,7 @@ def bench_reference(args, rank, world):
     res = one(args.workload, 40.0 if args.workload == "3d512" else 30.0)
     if res is None:
         return {"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}
-    subs = [s for s in args.subs.split(",") if s] if args.workload == "2d8192" else []
+    subs = [s for s in args.subs.split(",") if s] if (args.workload == "2d8192" and args.algo == "uf") else []
     if "3d512" in subs:
         r3 = one("3d512", 30.0)
         if r3 is not None:
@@ -868,8 +879,9 @@ def parse_args(argv=None):
     ap.add_argument("--subs", default="3d512,batch,serve",
                     help="with the 2d8192 headline: the other configurations measured in the same run, "
                          "as sub-records (empty string: none)")
-    ap.add_argument("--algo", default="uf", choices=["uf", "iter"],
-                    help="plain workloads: union-find form (default) or the iterative scan/analyze form")
+    ap.add_argument("--algo", default="uf", choices=["uf", "iter", "runs"],
+                    help="plain workloads: union-find form (default), the iterative scan/analyze form, or "
+                         "2D run equivalence (the runeq path, 4-connected)")
     ap.add_argument("--parts", type=int, default=4, help="slab2d on one GPU: number of slabs")
     ap.add_argument("--rates", default="100,300,1000,3000,5000", help="serve: Poisson rates (req/s)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg (and its parity check)")
@@ -901,7 +913,7 @@ def main():
         res = bench_slab(args, rank, world, local_rank)
     else:
         res = bench_plain(args, rank, world, local_rank, args.workload)
-        subs = [s for s in args.subs.split(",") if s] if args.workload == "2d8192" else []
+        subs = [s for s in args.subs.split(",") if s] if (args.workload == "2d8192" and args.algo == "uf") else []
         if subs:
             import torch
             res["sub"] = {}

@@ -47,9 +47,13 @@ enum {
     BE_ALGO_AUTO = 0, /* the autotuned choice (union-find unless the tuner measured otherwise) */
     BE_ALGO_UF = 1,   /* tile union-find in shared memory + global border merge */
     BE_ALGO_ITER = 2, /* the paper's iterative scan / analyze, with a device-side change flag */
-    BE_ALGO_PIXEL = 3 /* pixel-level label equivalence, the -a lbeq path (LabelingAlgs.cl:31-130,
-                         635-734): 2D 4-connectivity for BE_COH_4 / BE_COH_DEFAULT (the reference's
-                         default), 8 for BE_COH_8; 3D 26-connectivity */
+    BE_ALGO_PIXEL = 3, /* pixel-level label equivalence, the -a lbeq path (LabelingAlgs.cl:31-130,
+                          635-734): 2D 4-connectivity for BE_COH_4 / BE_COH_DEFAULT (the reference's
+                          default), 8 for BE_COH_8; 3D 26-connectivity */
+    BE_ALGO_RUNS = 4   /* 2D run equivalence, the -a runeq -g path (TOCLRunEquivLabeling,
+                          LabelingAlgs.cpp:1090-1268, RE* kernels LabelingAlgs.cl:325-616): runs of
+                          each row joined by column overlap -- 4-connectivity for BE_COH_4 /
+                          BE_COH_DEFAULT (the reference's runs), 8 for BE_COH_8; 2D only */
 };
 
 /* Connectivity selector, as the reference's TCoherence (LabelingTools.hpp:45-50). */

@@ -30,7 +30,7 @@ BE_OK = 0
 STATUS = {0: "BE_OK", 1: "BE_ERR_INVALID", 2: "BE_ERR_OOM", 3: "BE_ERR_NO_CONVERGENCE",
           4: "BE_ERR_CUDA", 5: "BE_ERR_TIMEOUT", 6: "BE_ERR_BUSY", 7: "BE_ERR_CANCELLED",
           8: "BE_ERR_TOO_LARGE"}
-ALGO_AUTO, ALGO_UF, ALGO_ITER, ALGO_PIXEL = 0, 1, 2, 3
+ALGO_AUTO, ALGO_UF, ALGO_ITER, ALGO_PIXEL, ALGO_RUNS = 0, 1, 2, 3, 4
 COH_4, COH_8, COH_DEFAULT = 0, 1, 2
 
 _lib = None
@@ -536,10 +536,10 @@ class RunEquivalence(Labeling):
     """The ``runeq -g`` slot (TOCLRunEquivLabeling, LabelingAlgs.cpp:1090-1268): the reference's
     run kernels join runs that overlap in a column -- 4-connectivity -- whatever coherence is
     asked for, and reject COH_4 themselves; so does this: COH_4 raises, anything else labels
-    4-connected on the pixel-level path."""
+    4-connected with the run-equivalence form (ALGO_RUNS)."""
 
     def __init__(self, device: int = 0):
-        super().__init__(ALGO_PIXEL, device)
+        super().__init__(ALGO_RUNS, device)
 
     def Label(self, pixels: np.ndarray, threads: int = 0, coh: int = COH_DEFAULT):
         if coh == COH_4:
@@ -572,7 +572,7 @@ class Labeling3D:
 ALGORITHMS = {
     "bleq": ("Block equivalence by Zavalishin et.al. 2016", ALGO_AUTO),
     "lbeq": ("Label equivalence by Kalentev et.al. 2012 (pixel level)", ALGO_PIXEL),
-    "runeq": ("Run equivalence by Bekhtin et.al. 2015 (4-connected, 2D only)", ALGO_PIXEL),
+    "runeq": ("Run equivalence by Bekhtin et.al. 2015 (4-connected, 2D only)", ALGO_RUNS),
 }
 
 

@@ -37,6 +37,9 @@ int cuda_error(be_ctx *ctx, cudaError_t e, const char *what)
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// The forms that run in the iterative graph (their count and error flag live in wsiter / iter_err).
+static bool iter_family(int algo) { return algo == BE_ALGO_ITER || algo == BE_ALGO_PIXEL || algo == BE_ALGO_RUNS; }
+
 Geometry geometry_2d() { return uf2d_geometry(0); }
 
 Geometry geometry_3d()
@@ -314,9 +317,9 @@ int be_label2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
         return set_error(c, BE_ERR_INVALID, "be_label2d: pitch smaller than the row");
     if (threshold < 0 || threshold > 255)
         return set_error(c, BE_ERR_INVALID, "be_label2d: threshold %d outside 0..255", threshold);
-    if (algo < BE_ALGO_AUTO || algo > BE_ALGO_PIXEL)
+    if (algo < BE_ALGO_AUTO || algo > BE_ALGO_RUNS)
         return set_error(c, BE_ERR_INVALID, "be_label2d: unknown algorithm %d", algo);
-    if (coh == BE_COH_4 && algo != BE_ALGO_PIXEL)
+    if (coh == BE_COH_4 && algo != BE_ALGO_PIXEL && algo != BE_ALGO_RUNS)
         return set_error(c, BE_ERR_INVALID, "be_label2d: block equivalence does not support 4-connectivity");
     if (coh != BE_COH_4 && coh != BE_COH_8 && coh != BE_COH_DEFAULT)
         return set_error(c, BE_ERR_INVALID, "be_label2d: unknown connectivity %d", coh);
@@ -328,6 +331,8 @@ int be_label2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
     c->last_algo = algo;
     if (algo == BE_ALGO_PIXEL) {
         rc = run_lbeq2d(c, in, in_pitch, rows, cols, threshold, coh == BE_COH_8, out, out_pitch, s);
+    } else if (algo == BE_ALGO_RUNS) {
+        rc = run_runeq2d(c, in, in_pitch, rows, cols, threshold, coh == BE_COH_8, out, out_pitch, s);
     } else if (algo == BE_ALGO_ITER) {
         rc = run_iter2d(c, in, in_pitch, rows, cols, threshold, out, out_pitch, s);
     } else {
@@ -347,11 +352,11 @@ int be_label2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int
     }
     if (rc) return rc;
     if (n_components) {
-        const int64_t *src = (algo == BE_ALGO_ITER || algo == BE_ALGO_PIXEL) ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
+        const int64_t *src = iter_family(algo) ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
         e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_error(c, e, "be_label2d sync");
-        if ((algo == BE_ALGO_ITER || algo == BE_ALGO_PIXEL) && c->iter_err && *c->iter_err)
+        if (iter_family(algo) && c->iter_err && *c->iter_err)
             return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label2d: iteration cap reached");
         *n_components = c->h_ncomp[0];
     }
@@ -369,7 +374,8 @@ int be_label3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
     if (threshold < 0 || threshold > 255)
         return set_error(c, BE_ERR_INVALID, "be_label3d: threshold %d outside 0..255", threshold);
     if (algo < BE_ALGO_AUTO || algo > BE_ALGO_PIXEL)
-        return set_error(c, BE_ERR_INVALID, "be_label3d: unknown algorithm %d", algo);
+        return set_error(c, BE_ERR_INVALID, algo == BE_ALGO_RUNS ? "be_label3d: run equivalence is 2D only"
+                                                                 : "be_label3d: unknown algorithm %d", algo);
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_error(c, e, "cudaSetDevice");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -397,11 +403,11 @@ int be_label3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
     }
     if (rc) return rc;
     if (n_components) {
-        const int64_t *src = (algo == BE_ALGO_ITER || algo == BE_ALGO_PIXEL) ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
+        const int64_t *src = iter_family(algo) ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
         e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_error(c, e, "be_label3d sync");
-        if ((algo == BE_ALGO_ITER || algo == BE_ALGO_PIXEL) && c->iter_err && *c->iter_err)
+        if (iter_family(algo) && c->iter_err && *c->iter_err)
             return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label3d: iteration cap reached");
         *n_components = c->h_ncomp[0];
     }
@@ -456,11 +462,11 @@ int be_label2d_host(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows
     e = cudaMemcpy2DAsync(out, out_pitch * sizeof(int32_t), c->d_out, dpo * sizeof(int32_t),
                           cols * sizeof(int32_t), rows, cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_error(c, e, "download");
-    const int64_t *src = (c->last_algo == BE_ALGO_ITER || c->last_algo == BE_ALGO_PIXEL) ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
+    const int64_t *src = iter_family(c->last_algo) ? c->wsiter.w.ncomp : c->ws2d.w.ncomp;
     e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(c, e, "be_label2d_host sync");
-    if ((c->last_algo == BE_ALGO_ITER || c->last_algo == BE_ALGO_PIXEL) && c->iter_err && *c->iter_err)
+    if (iter_family(c->last_algo) && c->iter_err && *c->iter_err)
         return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label2d_host: iteration cap reached");
     n = c->h_ncomp[0];
     if (n_components) *n_components = n;
@@ -496,11 +502,11 @@ int be_label3d_host(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_
     cudaEventRecord(c->ev1, s);
     e = cudaMemcpyAsync(out, c->d_out, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_error(c, e, "download");
-    const int64_t *src = (c->last_algo == BE_ALGO_ITER || c->last_algo == BE_ALGO_PIXEL) ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
+    const int64_t *src = iter_family(c->last_algo) ? c->wsiter.w.ncomp : c->ws3d.w.ncomp;
     e = cudaMemcpyAsync(c->h_ncomp, src, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(c, e, "be_label3d_host sync");
-    if ((c->last_algo == BE_ALGO_ITER || c->last_algo == BE_ALGO_PIXEL) && c->iter_err && *c->iter_err)
+    if (iter_family(c->last_algo) && c->iter_err && *c->iter_err)
         return set_error(c, BE_ERR_NO_CONVERGENCE, "be_label3d_host: iteration cap reached");
     if (n_components) *n_components = c->h_ncomp[0];
     if (elapsed_us) {

@@ -83,6 +83,8 @@ int run_lbeq2d(struct ::be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t 
                int conn8, int32_t *out, int64_t out_pitch, cudaStream_t s);
 int run_lbeq3d(struct ::be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int thr,
                int32_t *out, cudaStream_t s);
+int run_runeq2d(struct ::be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols, int thr,
+                int conn8, int32_t *out, int64_t out_pitch, cudaStream_t s);
 
 }  // namespace be
 
@@ -114,5 +116,5 @@ struct be_ctx {
     cudaEvent_t stage_ev[be::kStages + 1] = {};
     std::vector<be::TuneEntry> tune;  // autotuner decisions
     int last_algo = 1;                // algorithm the last label call actually ran
-    be_iter_graph iter_graph[4];      // iterative form: 2D / 3D blocks, 2D / 3D pixels
+    be_iter_graph iter_graph[5];      // iterative form: 2D / 3D blocks, 2D / 3D pixels, 2D runs
 };

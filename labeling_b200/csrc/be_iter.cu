@@ -512,6 +512,233 @@ __global__ void __launch_bounds__(NT) lq_final_3d(Lq3 g)
     g.out[p] = l;
 }
 
+// ---- run equivalence (-a runeq -g) -------------------------------------------------------------
+// The reference's TOCLRunEquivLabeling (LabelingAlgs.cpp:1090-1268, kernels RE* in
+// LabelingAlgs.cl:325-616): the nodes are the horizontal runs of each row; every run is given the
+// range of runs it overlaps in the row above and below; the Scan / Analyze loop then lowers each
+// run's root label to the smallest label among its neighbours and chases labels to their roots
+// until nothing changes; the final pass writes each run's label over its pixels.  The reference's
+// runs overlap by column only (4-connectivity); conn8 also joins runs that touch diagonally.
+// Differences, by design:
+//   * one warp per row finds the row's runs with ballot-free bit operations on 32-pixel words
+//     (foreground, run-start and run-end words, starts counted by a warp prefix sum), where the
+//     reference walks each row pixel by pixel in one thread (REFindRunsKernel);
+//   * a run's neighbour ranges come from the start-bit words in O(1) (count of run starts up to a
+//     column), not from a linear walk of the neighbouring row (FindNeibRuns);
+//   * the label is the run's index + 1 in raster order (row, then column), so roots end at each
+//     component's first run and its first pixel, and the output is canonical (first-pixel order);
+//   * the loop runs inside the iterative form's CUDA graph (device-side WHILE, iteration cap).
+struct Re2 {
+    const uint8_t *in;
+    int64_t pitch;
+    int32_t *out;
+    int64_t opitch;
+    int rows, cols, sx, thr, conn8;
+    int words;          // 32-pixel words per row
+    int rmax;           // run capacity per row: (cols + 1) / 2
+    uint32_t *fgb;      // [rows][words] foreground bits
+    uint32_t *stb;      // [rows][words] run-start bits
+    uint32_t *spre;     // [rows][words] run starts of the row before the word
+    uint32_t *nrun;     // [rows] runs of the row
+    int32_t *rl, *rr;   // [rows][rmax] first and last column of each run
+    uint32_t *lab;      // [rows][rmax] label: index + 1 of the run's current root run
+    uint4 *nb;          // [rows][rmax] overlapped runs (indices in their row): above first / last,
+                        //              below first / last (first > last: none)
+    uint32_t *rbits;    // root bitmap over first-pixel keys (y << sx) | x
+    uint32_t *ctl;
+    Work w;
+};
+
+// Foreground bits of 32 pixels starting at column x0 of row y (pixels past the row are 0).
+__device__ __forceinline__ uint32_t re_word(const Re2 &g, int y, int x0)
+{
+    const uint8_t *p = g.in + int64_t(y) * g.pitch + x0;
+    uint32_t m = 0;
+    if (x0 + 32 <= g.cols && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+        const uint4 a = __ldg(reinterpret_cast<const uint4 *>(p)), b = __ldg(reinterpret_cast<const uint4 *>(p) + 1);
+        const uint32_t v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) m |= uint32_t(((v[i] >> (8 * k)) & 0xFFu) > uint32_t(g.thr)) << (4 * i + k);
+    } else {
+        const int n = min(32, g.cols - x0);
+        for (int k = 0; k < n; ++k) m |= uint32_t(p[k] > g.thr) << k;
+    }
+    return m;
+}
+
+// One warp per row: the row's foreground / run-start words, the starts before each word, and the
+// runs' extents and initial labels.
+__global__ void __launch_bounds__(NT) re_rows(Re2 g)
+{
+    const int64_t gw = (int64_t(blockIdx.x) * NT + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= g.rows) return;   // whole warps leave together
+    const int y = int(gw);
+    uint32_t *fgb = g.fgb + int64_t(y) * g.words, *stb = g.stb + int64_t(y) * g.words;
+    uint32_t *spre = g.spre + int64_t(y) * g.words;
+    const int64_t rbase = int64_t(y) * g.rmax;
+    uint32_t carry = 0, offset = 0;   // last pixel of the previous chunk, starts before the chunk
+    for (int base = 0; base < g.words; base += 32) {
+        const int wd = base + lane;
+        const uint32_t f = wd < g.words ? re_word(g, y, 32 * wd) : 0u;
+        const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, f, 1);
+        const uint32_t prev = lane ? (up >> 31) : carry;
+        const uint32_t st = f & ~((f << 1) | prev);
+        uint32_t nxt = __shfl_down_sync(0xFFFFFFFFu, f, 1) & 1u;
+        if (lane == 31) nxt = (32 * (wd + 1) < g.cols) ? uint32_t(g.in[int64_t(y) * g.pitch + 32 * (wd + 1)] > g.thr) : 0u;
+        const uint32_t en = f & ~((f >> 1) | (nxt << 31));
+        // exclusive prefix of the starts over the warp
+        const uint32_t c = __popc(st);
+        uint32_t inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        const uint32_t pre = offset + inc - c;
+        if (wd < g.words) {
+            fgb[wd] = f;
+            stb[wd] = st;
+            spre[wd] = pre;
+            uint32_t b = st;
+            for (uint32_t k = pre; b; ++k) {
+                const int bit = __ffs(b) - 1;
+                b &= b - 1;
+                g.rl[rbase + k] = 32 * wd + bit;
+                g.lab[rbase + k] = uint32_t(rbase + k) + 1u;
+            }
+            // a run ends in this word: it is the last run started at or before that bit
+            b = en;
+            while (b) {
+                const int bit = __ffs(b) - 1;
+                b &= b - 1;
+                const uint32_t k = pre + __popc(st & (0xFFFFFFFFu >> (31 - bit))) - 1u;
+                g.rr[rbase + k] = 32 * wd + bit;
+            }
+        }
+        offset = __shfl_sync(0xFFFFFFFFu, pre + c, 31);
+        carry = __shfl_sync(0xFFFFFFFFu, f, 31) >> 31;
+    }
+    if (lane == 0) g.nrun[y] = offset;
+}
+
+// Runs of row y started at or before column x (x may be -1: none).
+__device__ __forceinline__ uint32_t re_starts_upto(const Re2 &g, int y, int x)
+{
+    if (x < 0) return 0u;
+    const int wd = x >> 5;
+    const int64_t i = int64_t(y) * g.words + wd;
+    return g.spre[i] + __popc(g.stb[i] & (0xFFFFFFFFu >> (31 - (x & 31))));
+}
+
+// Range of runs of row y that overlap columns [a, b] (clipped to the row): first > last when none.
+__device__ __forceinline__ uint2 re_range(const Re2 &g, int y, int a, int b)
+{
+    a = max(a, 0);
+    b = min(b, g.cols - 1);
+    if (a > b) return make_uint2(1u, 0u);
+    const bool fa = (g.fgb[int64_t(y) * g.words + (a >> 5)] >> (a & 31)) & 1u;
+    const uint32_t first = re_starts_upto(g, y, a) - (fa ? 1u : 0u);
+    const uint32_t last = re_starts_upto(g, y, b);   // one past the last
+    return last > first ? make_uint2(first, last - 1u) : make_uint2(1u, 0u);
+}
+
+__global__ void __launch_bounds__(NT) re_nbr(Re2 g)
+{
+    const int64_t i = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (i >= int64_t(g.rows) * g.rmax) return;
+    const int y = int(i / g.rmax), k = int(i - int64_t(y) * g.rmax);
+    if (uint32_t(k) >= g.nrun[y]) return;
+    const int a = g.rl[i] - g.conn8, b = g.rr[i] + g.conn8;
+    const uint2 up = y > 0 ? re_range(g, y - 1, a, b) : make_uint2(1u, 0u);
+    const uint2 dn = y + 1 < g.rows ? re_range(g, y + 1, a, b) : make_uint2(1u, 0u);
+    g.nb[i] = make_uint4(up.x, up.y, dn.x, dn.y);
+}
+
+// Scan: the smallest label among the overlapped runs lowers this run's root (REScanKernel,
+// LabelingAlgs.cl:555-577; atomicMin where the reference stores).
+__global__ void __launch_bounds__(NT) re_scan(Re2 g)
+{
+    const int64_t i = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (i >= int64_t(g.rows) * g.rmax) return;
+    const int y = int(i / g.rmax), k = int(i - int64_t(y) * g.rmax);
+    if (uint32_t(k) >= g.nrun[y]) return;
+    const uint32_t label = g.lab[i];
+    const uint4 r = g.nb[i];
+    uint32_t m = label;
+    for (uint32_t j = r.x; j <= r.y && r.x <= r.y; ++j) m = min(m, g.lab[int64_t(y - 1) * g.rmax + j]);
+    for (uint32_t j = r.z; j <= r.w && r.z <= r.w; ++j) m = min(m, g.lab[int64_t(y + 1) * g.rmax + j]);
+    if (m < label) {
+        atomicMin(&g.lab[label - 1], m);
+        g.ctl[0] = 1u;
+    }
+}
+
+// Analyze: every run's label chased to its root (REAnalizeKernel, LabelingAlgs.cl:581-601).
+__global__ void __launch_bounds__(NT) re_analyze(Re2 g)
+{
+    const int64_t i = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (i >= int64_t(g.rows) * g.rmax) return;
+    const int y = int(i / g.rmax), k = int(i - int64_t(y) * g.rmax);
+    if (uint32_t(k) >= g.nrun[y]) return;
+    uint32_t l = g.lab[i], c = g.lab[l - 1];
+    int steps = 0;
+    while (c != l) {
+        if (++steps > kChaseCap) {
+            g.ctl[2] = 1u;
+            return;
+        }
+        l = c;
+        c = g.lab[l - 1];
+    }
+    g.lab[i] = l;
+}
+
+// Roots mark their first pixel in the root bitmap.
+__global__ void __launch_bounds__(NT) re_mark(Re2 g)
+{
+    const int64_t i = int64_t(blockIdx.x) * NT + threadIdx.x;
+    if (i >= int64_t(g.rows) * g.rmax) return;
+    const int y = int(i / g.rmax), k = int(i - int64_t(y) * g.rmax);
+    if (uint32_t(k) >= g.nrun[y] || g.lab[i] != uint32_t(i) + 1u) return;
+    const uint32_t key = (uint32_t(y) << g.sx) | uint32_t(g.rl[i]);
+    atomicOr(&g.rbits[key >> 5], 1u << (key & 31));
+}
+
+// Final write (RELabelKernel, LabelingAlgs.cl:605-620): four pixels per thread; a foreground
+// pixel's run is the last run started at or before it, its label the canonical rank of the
+// run's root's first pixel.
+__global__ void __launch_bounds__(NT) re_final(Re2 g)
+{
+    const int64_t u = int64_t(blockIdx.x) * NT + threadIdx.x;
+    const int units = (g.cols + 3) >> 2;
+    if (u >= int64_t(g.rows) * units) return;
+    const int y = int(u / units), x0 = 4 * int(u - int64_t(y) * units);
+    const uint32_t f = g.fgb[int64_t(y) * g.words + (x0 >> 5)] >> (x0 & 31);
+    int v[4] = {0, 0, 0, 0};
+    uint32_t run = 0xFFFFFFFFu, lbl = 0;
+    for (int q = 0; q < 4 && x0 + q < g.cols; ++q) {
+        if (!((f >> q) & 1u)) continue;
+        const uint32_t r = re_starts_upto(g, y, x0 + q) - 1u;
+        if (r != run) {
+            run = r;
+            const uint32_t root = g.lab[int64_t(y) * g.rmax + r] - 1u;
+            const uint32_t ry = root / uint32_t(g.rmax);
+            const uint32_t key = (ry << g.sx) | uint32_t(g.rl[root]);
+            lbl = 1u + g.w.segpref[key >> 5] + __popc(g.rbits[key >> 5] & ((1u << (key & 31)) - 1u));
+        }
+        v[q] = int(lbl);
+    }
+    int32_t *dst = g.out + int64_t(y) * g.opitch + x0;
+    if (x0 + 4 <= g.cols && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0)) {
+        *reinterpret_cast<int4 *>(dst) = make_int4(v[0], v[1], v[2], v[3]);
+    } else {
+        for (int q = 0; q < 4 && x0 + q < g.cols; ++q) dst[q] = v[q];
+    }
+}
+
 unsigned nblk(int64_t n) { return unsigned((n + NT - 1) / NT); }
 
 int ceil_log2(int v)
@@ -539,10 +766,11 @@ cudaError_t add_kernel(cudaGraph_t graph, cudaGraphNode_t *node, cudaGraphNode_t
 // Scratch of the iterative form: block labels, masks, connectivity, root bitmap and the segment
 // workspace (over bitmap words), carved from the context's iteration buffer.
 int iter_scratch(be_ctx *c, int64_t nblocks, size_t conn_bytes, int64_t nwords, char **lab, char **mk,
-                 char **conn, char **rbits, char **ctl)
+                 char **conn, char **rbits, char **ctl, size_t extra_bytes = 0, char **extra = nullptr)
 {
     auto al = [](size_t v) { return (v + 255) / 256 * 256; };
-    const size_t need = al(nblocks * 4) + al(nblocks) + al(nblocks * conn_bytes) + al(nwords * 4) + 256;
+    const size_t need = al(nblocks * 4) + al(nblocks) + al(nblocks * conn_bytes) + al(nwords * 4) + 256 +
+                        al(extra_bytes);
     if (need > c->iter_bytes) {
         if (c->iter_base) cudaFree(c->iter_base);
         c->iter_base = nullptr;
@@ -556,7 +784,8 @@ int iter_scratch(be_ctx *c, int64_t nblocks, size_t conn_bytes, int64_t nwords, 
     *mk = p; p += al(nblocks);
     *conn = p; p += al(nblocks * conn_bytes);
     *rbits = p; p += al(nwords * 4);
-    *ctl = p;
+    *ctl = p; p += 256;
+    if (extra) *extra = p;
     if (!c->iter_err) {
         cudaError_t e = cudaMallocHost(&c->iter_err, 16);
         if (e != cudaSuccess) return cuda_error(c, e, "cudaMallocHost(iteration flag)");
@@ -570,6 +799,7 @@ void blank_io(It2 &g) { g.in = nullptr; g.out = nullptr; g.pitch = g.opitch = 0;
 void blank_io(It3 &g) { g.in = nullptr; g.out = nullptr; g.thr = 0; }
 void blank_io(Lq2 &g) { g.in = nullptr; g.out = nullptr; g.pitch = g.opitch = 0; g.thr = 0; }
 void blank_io(Lq3 &g) { g.in = nullptr; g.out = nullptr; g.thr = 0; }
+void blank_io(Re2 &g) { g.in = nullptr; g.out = nullptr; g.pitch = g.opitch = 0; g.thr = 0; }
 
 template <class G>
 cudaError_t set_kernel_args(cudaGraphExec_t exec, cudaGraphNode_t node, void *fn, unsigned grid, G &g)
@@ -590,21 +820,22 @@ cudaError_t set_kernel_args(cudaGraphExec_t exec, cudaGraphNode_t node, void *fn
 // updated, while the sizes and scratch buffers stay the same.
 template <class G, class FI, class FC, class FS, class FA, class FM, class FF>
 int run_graph(be_ctx *c, int kind, G g, int64_t nblocks, int64_t nfinal, int64_t nwords, FI f_init, FC f_conn,
-              FS f_scan, FA f_an, FM f_mark, FF f_final, cudaStream_t s)
+              FS f_scan, FA f_an, FM f_mark, FF f_final, cudaStream_t s, int64_t ninit = -1)
 {
+    if (ninit < 0) ninit = nblocks;   // threads of the init launch (the others run over nblocks)
     be_iter_graph &cache = c->iter_graph[kind];
-    std::vector<unsigned char> key(sizeof(G) + 4 * sizeof(int64_t));
+    std::vector<unsigned char> key(sizeof(G) + 5 * sizeof(int64_t));
     {
         G k;
         std::memcpy(&k, &g, sizeof(G));
         blank_io(k);
         std::memcpy(key.data(), &k, sizeof(G));
-        const int64_t extra[4] = {nblocks, nfinal, nwords, int64_t(reinterpret_cast<uintptr_t>(c->iter_err))};
+        const int64_t extra[5] = {nblocks, nfinal, nwords, int64_t(reinterpret_cast<uintptr_t>(c->iter_err)), ninit};
         std::memcpy(key.data() + sizeof(G), extra, sizeof(extra));
     }
     cudaError_t e;
     if (cache.exec && cache.key == key) {
-        e = set_kernel_args(cache.exec, cache.init, reinterpret_cast<void *>(f_init), nblk(nblocks), g);
+        e = set_kernel_args(cache.exec, cache.init, reinterpret_cast<void *>(f_init), nblk(ninit), g);
         if (e == cudaSuccess)
             e = set_kernel_args(cache.exec, cache.fin, reinterpret_cast<void *>(f_final), nblk(nfinal), g);
         if (e == cudaSuccess) e = cudaGraphLaunch(cache.exec, s);
@@ -640,7 +871,7 @@ int run_graph(be_ctx *c, int kind, G g, int64_t nblocks, int64_t nfinal, int64_t
         m2.height = 1;
         e = chain(cudaGraphAddMemsetNode(&n, graph, &prev, 1, &m2));
     }
-    if (e == cudaSuccess) e = chain(add_kernel(graph, &n, prev, f_init, nblk(nblocks), NT, g));
+    if (e == cudaSuccess) e = chain(add_kernel(graph, &n, prev, f_init, nblk(ninit), NT, g));
     if (e == cudaSuccess) n_init = n;
     if (e == cudaSuccess && f_conn) e = chain(add_kernel(graph, &n, prev, f_conn, nblk(nblocks), NT, g));
     cudaGraphConditionalHandle h;
@@ -797,6 +1028,44 @@ int run_lbeq3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
     g.w.queue = nullptr;
     return run_graph(c, 3, g, n, n, nwords, lq_init_3d, (void (*)(Lq3)) nullptr, lq_scan_3d, lq_analyze_3d,
                      lq_mark_3d, lq_final_3d, s);
+}
+
+int run_runeq2d(be_ctx *c, const uint8_t *in, int64_t in_pitch, int32_t rows, int32_t cols, int thr, int conn8,
+                int32_t *out, int64_t out_pitch, cudaStream_t s)
+{
+    Re2 g{};
+    g.in = in; g.pitch = in_pitch; g.out = out; g.opitch = out_pitch;
+    g.rows = rows; g.cols = cols; g.thr = thr; g.conn8 = conn8 ? 1 : 0;
+    g.sx = ceil_log2(cols);
+    g.words = (cols + 31) / 32;
+    g.rmax = (cols + 1) / 2;
+    const int64_t keyspace = int64_t(rows) << g.sx;
+    if (keyspace >= (int64_t(1) << 31))
+        return set_error(c, BE_ERR_INVALID, "run equivalence: %d x %d exceeds its key space", rows, cols);
+    const int64_t nruns = int64_t(rows) * g.rmax, nwords = (keyspace + 31) / 32;
+    const int64_t rw = int64_t(rows) * g.words;
+    auto al = [](size_t v) { return (v + 255) / 256 * 256; };
+    const size_t extra = 3 * al(size_t(rw) * 4) + al(size_t(rows) * 4) + 2 * al(size_t(nruns) * 4);
+    char *lab, *mk, *nb, *rb, *ctl, *ex;
+    int rc = iter_scratch(c, nruns, sizeof(uint4), nwords, &lab, &mk, &nb, &rb, &ctl, extra, &ex);
+    if (rc) return rc;
+    rc = c->wsiter.ensure(c, geometry_2d(), 0, nwords, 1);
+    if (rc) return rc;
+    g.lab = reinterpret_cast<uint32_t *>(lab);
+    g.nb = reinterpret_cast<uint4 *>(nb);
+    g.rbits = reinterpret_cast<uint32_t *>(rb);
+    g.ctl = reinterpret_cast<uint32_t *>(ctl);
+    g.fgb = reinterpret_cast<uint32_t *>(ex); ex += al(size_t(rw) * 4);
+    g.stb = reinterpret_cast<uint32_t *>(ex); ex += al(size_t(rw) * 4);
+    g.spre = reinterpret_cast<uint32_t *>(ex); ex += al(size_t(rw) * 4);
+    g.nrun = reinterpret_cast<uint32_t *>(ex); ex += al(size_t(rows) * 4);
+    g.rl = reinterpret_cast<int32_t *>(ex); ex += al(size_t(nruns) * 4);
+    g.rr = reinterpret_cast<int32_t *>(ex);
+    g.w = c->wsiter.w;
+    g.w.n_tiles = 0;
+    g.w.queue = nullptr;
+    return run_graph(c, 4, g, nruns, int64_t(rows) * ((cols + 3) / 4), nwords, re_rows, re_nbr, re_scan, re_analyze,
+                     re_mark, re_final, s, int64_t(rows) * 32);
 }
 
 }  // namespace be

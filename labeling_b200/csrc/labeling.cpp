@@ -92,7 +92,7 @@ TTime TCudaBlockEquivalence3D::Label(const TImage &pixels, TLabelImage &labels, 
     return TTime(us);
 }
 
-TCudaRunEquivalence::TCudaRunEquivalence(bool runOnGPU, int device) : inner_(runOnGPU, BE_ALGO_PIXEL, device) {}
+TCudaRunEquivalence::TCudaRunEquivalence(bool runOnGPU, int device) : inner_(runOnGPU, BE_ALGO_RUNS, device) {}
 
 TTime TCudaRunEquivalence::Label(const TImage &pixels, TLabelImage &labels, char threads, TCoherence coh)
 {

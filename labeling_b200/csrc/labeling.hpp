@@ -91,7 +91,8 @@ private:
 // GPU run equivalence, 2D (the `runeq` GPU slot; replaces TOCLRunEquivLabeling,
 // LabelingAlgs.cpp:1090-1268).  The reference's run kernels join runs that overlap in a column,
 // which is 4-connectivity, whatever coherence is asked for, and it rejects COH_4 itself; this
-// slot keeps both: COH_4 throws, anything else labels 4-connected, on the pixel-level path.
+// slot keeps both: COH_4 throws, anything else labels 4-connected, with the run-equivalence form
+// (BE_ALGO_RUNS).
 class TCudaRunEquivalence final : public ILabeling {
 public:
     explicit TCudaRunEquivalence(bool runOnGPU = true, int device = 0);

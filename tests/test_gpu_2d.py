@@ -146,12 +146,13 @@ def test_pixel_label_equivalence_lbeq(ctx, golden, conn8):
 
 def test_run_equivalence_slot_matches_reference_kernels(ctx, golden):
     """-a runeq -g: the reference's run kernels (golden outputs) give 4-connected components; the
-    slot labels them on the pixel path with 4-connectivity and rejects COH_4 as the reference."""
+    slot labels them with the run-equivalence form, 4-connected, and rejects COH_4 as the
+    reference does."""
     import labeling_b200 as be
     for (dim, name), c in golden.items():
         if dim != "2d":
             continue
-        lab, n, _ = be.label2d_host(ctx, c["img"], int(c["thr"]), be.ALGO_PIXEL, be.COH_4)
+        lab, n, _ = be.label2d_host(ctx, c["img"], int(c["thr"]), be.ALGO_RUNS, be.COH_4)
         want, k = O.canon(c["runeq"])
         assert n == k and np.array_equal(lab, want), name
     lab_alg = be.make_labeler("runeq")
@@ -190,3 +191,53 @@ def test_iterative_graph_cache_reuse(ctx):
         out = torch.empty(shape, dtype=torch.int32, device="cuda")
         assert be.label3d(ctx, d, out, threshold=thr, algo=be.ALGO_ITER) == k
         assert np.array_equal(out.cpu().numpy(), ref), (shape, thr)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_run_equivalence_form_vs_oracle(ctx, seed):
+    """The run-equivalence form (runs per row, overlap ranges, Scan / Analyze) on random shapes,
+    pitches and thresholds: 4-connectivity (BE_COH_4 and the default) and 8 (BE_COH_8), exact."""
+    import labeling_b200 as be
+    rng = np.random.default_rng(300 + seed)
+    h = int(rng.choice([1, 2, 3, 31, 32, 33, 100, 257]))
+    w = int(rng.choice([1, 2, 31, 32, 33, 63, 64, 65, 500, 1025]))
+    img = rng.integers(0, 256, (h, w)).astype(np.uint8)
+    thr = int(rng.choice([0, 100, 200]))
+    for coh, conn8 in ((be.COH_4, False), (be.COH_DEFAULT, False), (be.COH_8, True)):
+        ref, k = O.ccl2d(img, thr, conn8)
+        for pad, off in ((0, 0), (7, 5)):
+            import torch
+            buf = torch.zeros(h * (w + pad) + off + 64, dtype=torch.uint8, device="cuda")
+            view = buf[off:off + h * (w + pad)].view(h, w + pad)[:, :w]
+            view.copy_(torch.from_numpy(img).cuda())
+            out = torch.full((h, w + pad), -7, dtype=torch.int32, device="cuda")[:, :w]
+            n = be.label2d(ctx, view, out, threshold=thr, algo=be.ALGO_RUNS, coh=coh)
+            assert n == k and np.array_equal(out.cpu().numpy(), ref), (h, w, thr, coh, pad, off)
+
+
+@pytest.mark.parametrize("family", ["serpentine", "spiral", "bern0.5"])
+def test_run_equivalence_long_paths(ctx, family):
+    """Paths that need many Scan / Analyze rounds (one serpentine or spiral run chain) and dense
+    noise, 2048 x 2048, both connectivities, exact; full-size images are in test_gpu_full.py."""
+    import labeling_b200 as be
+    from labeling_b200 import workloads as W
+    img = W.family_8192(family, seed=5, side=2048)
+    for coh, conn8 in ((be.COH_4, False), (be.COH_8, True)):
+        ref, k = O.ccl2d(img, 0, conn8)
+        lab, n = run2d(ctx, img, 0, algo=be.ALGO_RUNS) if coh == be.COH_4 else (None, None)
+        if coh == be.COH_8:
+            import torch
+            d = torch.from_numpy(img).cuda()
+            o = torch.empty(img.shape, dtype=torch.int32, device="cuda")
+            n = be.label2d(ctx, d, o, algo=be.ALGO_RUNS, coh=be.COH_8)
+            lab = o.cpu().numpy()
+        assert n == k and np.array_equal(lab, ref), (family, coh)
+
+
+def test_run_equivalence_rejects_3d(ctx):
+    import torch
+    import labeling_b200 as be
+    v = torch.zeros((4, 5, 6), dtype=torch.uint8, device="cuda")
+    o = torch.zeros((4, 5, 6), dtype=torch.int32, device="cuda")
+    with pytest.raises(be.BEError):
+        be.label3d(ctx, v, o, algo=be.ALGO_RUNS)
