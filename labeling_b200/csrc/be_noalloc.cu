@@ -48,9 +48,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void *g_addr[kMaxDevices] = {};
+int g_sms[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device (looked up once per device).
-int scratch_address(void **out)
+// Device address of the scratch array on the current device, and the device's SM count (the
+// launch sizes some grids by it); both looked up once per device.
+int scratch_address(void **out, int *sms)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BE_ERR_CUDA;
@@ -60,9 +62,14 @@ int scratch_address(void **out)
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return BE_ERR_CUDA;
         if (be::layout_work(be::geometry_2d(), kMaxTiles, kMaxSegs, 1, nullptr, nullptr) > kScratchBytes)
             return BE_ERR_CUDA;
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+            return BE_ERR_CUDA;
+        g_sms[dev] = n;
         g_addr[dev] = p;
     }
     *out = g_addr[dev];
+    *sms = g_sms[dev];
     return BE_OK;
 }
 
@@ -81,7 +88,8 @@ extern "C" int be_label2d_noalloc(const uint8_t *in, int64_t in_pitch, int32_t r
     const int64_t n_segs = int64_t(rows) * im.tiles_x;
     if (n_tiles > kMaxTiles || n_segs > kMaxSegs) return BE_ERR_TOO_LARGE;
     void *base = nullptr;
-    int rc = scratch_address(&base);
+    int sms = 0;
+    int rc = scratch_address(&base, &sms);
     if (rc) return rc;
     be::Work w;
     be::layout_work(be::geometry_2d(), kMaxTiles, kMaxSegs, 1, static_cast<char *>(base), &w);
@@ -91,7 +99,7 @@ extern "C" int be_label2d_noalloc(const uint8_t *in, int64_t in_pitch, int32_t r
     w.n_imgs = 1;
     be::ImgList2D L{nullptr, 1, im};
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (be::uf2d_launch(0, L, w, 0, false, s) != cudaSuccess) return BE_ERR_CUDA;
+    if (be::uf2d_launch(0, L, w, sms, false, s) != cudaSuccess) return BE_ERR_CUDA;
     if (n_components) {
         if (cudaMemcpyAsync(n_components, w.ncomp, sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)

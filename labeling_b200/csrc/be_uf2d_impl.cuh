@@ -258,33 +258,31 @@ __global__ void __launch_bounds__(K1_NT, 7) k_tile_local_2d(ImgList2D L, Work w)
         WHC[tid] = hc;
         WS[tid] = S;
         WCS[tid] = CSc;
-        // Slots of the runs that start here: the first block with a top pixel, else the start.
+        // Slot keys across words: a run that goes on into later words of its row takes its slot
+        // from the first top pixel there when its own part has none.  Each word reports the first
+        // top pixel of the run carried into it (0xFF: none) and whether that run also goes on past
+        // the word (0x100); the word holding the run's start reads them with shuffles inside the
+        // row's lanes, so every slot is complete when it is first written.
+        const uint32_t cbrk = ~hc;
+        const uint32_t ctm = cin ? (Tw & ((2u << (cbrk ? uint32_t(__ffs(cbrk) - 1) : 31u)) - 1u)) : 0u;
+        const uint32_t mine = (ctm ? uint32_t(32 * q + __ffs(ctm) - 1) : 0xFFu) | ((cin && !cbrk) ? 0x100u : 0u);
+        uint32_t tail = 0xFFu;   // first top pixel of this word's last run in the words after it
         {
-            uint32_t ss = S;
-            while (ss) {
-                const uint32_t s0 = __ffs(ss) - 1;
-                ss &= ss - 1;
-                const uint32_t from = ~0u << s0;
-                const uint32_t brk = ~hc & from;
-                const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
-                const uint32_t tm = Tw & from & ((2u << e) - 1u);
-                const uint32_t key = tm ? sbase + 32 * q + (__ffs(tm) - 1) : sbase + TBW + 32 * q + s0;
-                const uint32_t x = rbase + 32 * q + s0;
-                P[sw(x)] = (key << 12) | x;
+            bool open = (hc >> 31) & 1u;   // the word's last run goes on into the next word
+#pragma unroll
+            for (int d = 1; d < WPR; ++d) {
+                const uint32_t pj = __shfl_down_sync(0xFFFFFFFFu, mine, d, WPR);
+                if (open && q + d < WPR) {
+                    if ((pj & 0xFFu) != 0xFFu) {
+                        tail = pj & 0xFFu;
+                        open = false;
+                    } else if (!(pj & 0x100u)) {
+                        open = false;
+                    }
+                }
             }
         }
-        __syncthreads();
-        // A run that entered from the left and has a top pixel here may have a smaller slot.
-        if (cin) {
-            const uint32_t brk = ~hc;
-            const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
-            const uint32_t tm = Tw & ((2u << e) - 1u);
-            if (tm && GUARD(w, CSc < uint32_t(TBW), 111, CSc)) {
-                const uint32_t x = rbase + (CSc & (TBW - 1));
-                atomicMin(&P[sw(x)], ((sbase + 32 * q + (__ffs(tm) - 1)) << 12) | x);
-            }
-        }
-        __syncthreads();   // slots final before any union reads them
+        __syncthreads();   // words of every row written
 
         // Phase B: links to the block row above.  For block b of this row: N (straight up, a top
         // pixel over a bottom pixel), NW (top-left pixel to the bottom-right pixel of b - 1 above)
@@ -330,59 +328,72 @@ __global__ void __launch_bounds__(K1_NT, 7) k_tile_local_2d(ImgList2D L, Work w)
         };
         const uint32_t ubase = rbase - TBW + 32 * q, abase = rbase + 32 * q;
 
-        // Forest: a run that starts in this word takes its first kept link in this word as its
-        // parent.  The parent is in the row above, whose slots are all smaller than this row's, so
-        // a plain store links it (no atomic, no cycle possible).  The parent's entry copied here
-        // is its own root entry or, when its owner has already linked it the same way, the entry
-        // of its own parent: an ancestor either way.  These links leave the queue; the union-find
-        // below walks the forest's paths like any other (path halving), and the flatten pass
-        // compresses them.  (Pointer jumping over the forest first was measured slower.)
+        // Every run that starts in this word gets its entry.  A run with a kept link in this word
+        // takes the first one as its parent: the parent is in the row above, whose slots are all
+        // smaller than this row's, so a plain store links it (no atomic, no cycle possible).  Its
+        // entry holds key 0 -- the smallest value, so no atomicMin of a union ever changes it and
+        // unions walk on to the parent; only a root's key is ever compared.  Any other run is a
+        // root for now: (slot << 12) | itself, the slot being its first block with a top pixel
+        // (this word, else the words after it), else its start.  These forest links leave the
+        // queue; the union-find below walks the forest like any other path (path halving), and
+        // the flatten pass compresses it.  (Pointer jumping over the forest first was measured
+        // slower.)
         {
             uint32_t ss = S;
             while (ss) {
                 const uint32_t s0 = __ffs(ss) - 1;
                 ss &= ss - 1;
-                const uint32_t brk = ~hc & (~0u << s0);
+                const uint32_t from = ~0u << s0;
+                const uint32_t brk = ~hc & from;
                 const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
-                const uint32_t lk = (Nm | NWm | NEm) & (~0u << s0) & (0xFFFFFFFFu >> (31u - e));
-                if (!lk) continue;
-                const uint32_t b = __ffs(lk) - 1, bit = 1u << b;
-                uint32_t tgt;
-                if (Nm & bit) {
-                    tgt = ubase + b;
-                    Nm &= ~bit;
-                } else if (NWm & bit) {
-                    tgt = ubase + b - 1;
-                    NWm &= ~bit;
+                const uint32_t span = from & (0xFFFFFFFFu >> (31u - e));
+                const uint32_t lk = (Nm | NWm | NEm) & span;
+                const uint32_t x = abase + s0;
+                if (lk) {
+                    const uint32_t b = __ffs(lk) - 1, bit = 1u << b;
+                    uint32_t tgt;
+                    if (Nm & bit) {
+                        tgt = ubase + b;
+                        Nm &= ~bit;
+                    } else if (NWm & bit) {
+                        tgt = ubase + b - 1;
+                        NWm &= ~bit;
+                    } else {
+                        tgt = ubase + b + 1;
+                        NEm &= ~bit;
+                    }
+                    P[sw(x)] = start_of(tgt);   // key 0
                 } else {
-                    tgt = ubase + b + 1;
-                    NEm &= ~bit;
+                    const uint32_t tm = Tw & span;
+                    uint32_t key = sbase + TBW + 32 * q + s0;
+                    if (tm) key = sbase + 32 * q + (__ffs(tm) - 1);
+                    else if (brk == 0 && tail != 0xFFu) key = sbase + tail;
+                    P[sw(x)] = (key << 12) | x;
                 }
-                P[sw(abase + s0)] = P[sw(start_of(tgt))];
             }
         }
-        __syncthreads();
         // The remaining links are unions.  The queue holds the two blocks of each link; their run
-        // starts are looked up by the merging lanes, which share that work evenly.
+        // starts are looked up by the merging lanes, which share that work evenly.  Links past the
+        // queue's capacity are merged in place by their own thread once every entry is written.
         const uint32_t n = __popc(Nm) + __popc(NWm) + __popc(NEm);
-        uint32_t pos = warp_reserve(&mqn, n);
-        {
-            auto push = [&](uint32_t a, uint32_t b) {
-                if (pos < uint32_t(MQCAP)) MQ[pos] = (a << 16) | b;
-                else eunion(P, start_of(a), start_of(b));   // queue full: merge in place
-                ++pos;
-            };
+        const uint32_t pos0 = warp_reserve(&mqn, n);
+        auto each_link = [&](auto &&f) {
+            uint32_t pos = pos0;
             uint32_t todo = Nm | NWm | NEm;
             while (todo) {
                 const uint32_t b = __ffs(todo) - 1;
                 todo &= todo - 1;
                 const uint32_t bit = 1u << b;
                 const uint32_t a = abase + b;
-                if (Nm & bit) push(a, ubase + b);
-                if (NWm & bit) push(a, ubase + b - 1);   // b = 0: the last block of the word before
-                if (NEm & bit) push(a, ubase + b + 1);   // b = 31: the first block of the word after
+                if (Nm & bit) f(pos++, a, ubase + b);
+                if (NWm & bit) f(pos++, a, ubase + b - 1);   // b = 0: the last block of the word before
+                if (NEm & bit) f(pos++, a, ubase + b + 1);   // b = 31: the first block of the word after
             }
-        }
+        };
+        if (pos0 < uint32_t(MQCAP))
+            each_link([&](uint32_t pos, uint32_t a, uint32_t b) {
+                if (pos < uint32_t(MQCAP)) MQ[pos] = (a << 16) | b;
+            });
         __syncthreads();
         {
             const uint32_t nq = min(mqn, uint32_t(MQCAP));
@@ -390,6 +401,10 @@ __global__ void __launch_bounds__(K1_NT, 7) k_tile_local_2d(ImgList2D L, Work w)
             // rows, are merged one after another by one thread instead of racing on the same roots.
             const uint32_t per = (nq + K1_NT - 1) / K1_NT, lo = min(nq, uint32_t(tid) * per), hi = min(nq, lo + per);
             for (uint32_t i = lo; i < hi; ++i) eunion(P, start_of(MQ[i] >> 16), start_of(MQ[i] & 0xFFFFu));
+            if (pos0 + n > uint32_t(MQCAP))
+                each_link([&](uint32_t pos, uint32_t a, uint32_t b) {
+                    if (pos >= uint32_t(MQCAP)) eunion(P, start_of(a), start_of(b));
+                });
         }
         __syncthreads();
 
@@ -537,19 +552,22 @@ __device__ void gunion2d(const Img2D &im, Work &w, uint32_t a, uint32_t b)
 
 }  // namespace
 
-constexpr int K2_NT = TBH + TBW;
-constexpr int kGQ2 = 512;                      // queued global unions per tile (more are done at once)
+constexpr int K2_NP = TBH + TBW;               // border positions a merge CTA looks at
+constexpr int K2_NT = 64;                      // threads of a merge CTA (small: many tiles per SM)
+constexpr int kGQ2 = 256;                      // queued global unions per tile (more are done at once)
 constexpr int SR = MAXB;                       // local index of the staged right column
 constexpr int SD = MAXB + TBH;                 // local index of the staged bottom row (column -1 first)
 constexpr int NLOC2 = MAXB + TBH + TBW + 2;    // local union-find size
 
-// One thread per right-border and bottom-border position.  The border entries across the right
-// border (the next tile's left column) and the bottom border (the top row of the tile below,
-// widened by one block into the two diagonal tiles) are staged in shared memory with the global
-// node id they belong to.  A CTA-local union-find over this tile's nodes and the staged positions
-// (neighbouring staged positions of one node merged first) filters the pairs: only a pair that
-// joins two local sets goes on to the global union-find, from a shared queue once all of the
-// tile's pairs are seen.
+// Positions p < TBH are the right border's rows, the others the bottom border's columns
+// (p - TBH).  The border entries across the right border (the next tile's left column) and the
+// bottom border (the top row of the tile below, widened by one block into the two diagonal tiles)
+// are staged in shared memory with the global node id they belong to.  A CTA-local union-find over
+// this tile's nodes and the staged positions (neighbouring staged positions of one node merged
+// first) filters the pairs: only a pair that joins two local sets goes on to the global
+// union-find, from a shared queue once all of the tile's pairs are seen.  The merge is bound by
+// the latency of those global unions (dependent L2 round trips), so a CTA is two warps that loop
+// over the positions: many tiles are in flight on each SM at once.
 __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
 {
     grid_dep_wait();
@@ -558,6 +576,7 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
     __shared__ uint32_t lp[NLOC2];
     __shared__ uint32_t sid[TBH + TBW + 2];   // staged global node ids (kNone = none)
     __shared__ uint8_t smk[TBH + TBW + 2];    // staged masks
+    __shared__ uint16_t own[K2_NP];           // this tile's own border entries
     __shared__ uint2 gq[kGQ2];
     __shared__ uint32_t nq;
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
@@ -567,56 +586,63 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
         const int ty = int(lt / im.tiles_x), tx = int(lt - int64_t(ty) * im.tiles_x);
         const int nbr = (min(TH, im.rows - ty * TH) + 1) >> 1;
         const int nbc = (min(TW, im.cols - tx * TW) + 1) >> 1;
-        const int p = threadIdx.x;
         const uint16_t *pe = w.perim;
-        // This position's own border entry, loaded with the staging loads (the pairs use it).
-        uint32_t A = 0;
-        if (p < TBH) {
-            if (p < nbr && tx + 1 < im.tiles_x) A = pe[t * NPERIM + 2 * TBW + TBH + p];
-        } else if (p - TBH < nbc && ty + 1 < im.tiles_y) {
-            A = pe[t * NPERIM + TBW + (p - TBH)];
-        }
-        for (int i = p; i < NLOC2; i += K2_NT) lp[i] = uint32_t(i);
-        if (p == 0) nq = 0;
-        // Stage: thread p < TBH takes right-column row p; the others take bottom-row column
-        // p - TBH, and the first of them also columns -1 and nbc.
-        {
-            auto stage = [&](int k, int64_t t2, int pos) {
-                const uint32_t B = pe[t2 * NPERIM + pos];
-                sid[k] = B ? uint32_t(t2 * MAXB + (B >> 4)) : kNone;
-                smk[k] = uint8_t(B & 15u);
-            };
+        for (int i = threadIdx.x; i < NLOC2; i += K2_NT) lp[i] = uint32_t(i);
+        if (threadIdx.x == 0) nq = 0;
+        // Stage: position p < TBH stages right-column row p; the others bottom-row column p - TBH,
+        // and the first two of those also columns -1 and TBW.  Each position's own entry is loaded
+        // with the staging loads.
+        auto stage = [&](int k, int64_t t2, int pos) {
+            const uint32_t B = pe[t2 * NPERIM + pos];
+            sid[k] = B ? uint32_t(t2 * MAXB + (B >> 4)) : kNone;
+            smk[k] = uint8_t(B & 15u);
+        };
+        for (int p = threadIdx.x; p < K2_NP; p += K2_NT) {
+            uint16_t A = 0;
             if (p < TBH) {
-                if (p < nbr && tx + 1 < im.tiles_x) stage(p, t + 1, 2 * TBW + p);
-                else { sid[p] = kNone; smk[p] = 0; }
+                if (p < nbr && tx + 1 < im.tiles_x) {
+                    A = pe[t * NPERIM + 2 * TBW + TBH + p];
+                    stage(p, t + 1, 2 * TBW + p);
+                } else {
+                    sid[p] = kNone;
+                    smk[p] = 0;
+                }
             } else {
                 const int c = p - TBH;
                 const int k = TBH + 1 + c;
-                if (c < nbc && ty + 1 < im.tiles_y) stage(k, t + im.tiles_x, c);
-                else { sid[k] = kNone; smk[k] = 0; }
+                if (c < nbc && ty + 1 < im.tiles_y) {
+                    A = pe[t * NPERIM + TBW + c];
+                    stage(k, t + im.tiles_x, c);
+                } else {
+                    sid[k] = kNone;
+                    smk[k] = 0;
+                }
                 if (c == 0) {
                     if (tx > 0 && ty + 1 < im.tiles_y) stage(TBH, t + im.tiles_x - 1, TBW - 1);
                     else { sid[TBH] = kNone; smk[TBH] = 0; }
                 }
                 if (c == 1) {
                     // column TBW: block 0 of the tile below-right (a tile with a right neighbour is
-                    // full-width; a narrower tile's column nbc is staged empty by its own thread)
+                    // full-width; a narrower tile's column nbc is staged empty by its own position)
                     if (nbc == TBW && tx + 1 < im.tiles_x && ty + 1 < im.tiles_y)
                         stage(TBH + TBW + 1, t + im.tiles_x + 1, 0);
                     else { sid[TBH + TBW + 1] = kNone; smk[TBH + TBW + 1] = 0; }
                 }
             }
+            own[p] = A;
         }
         __syncthreads();
         // Neighbouring staged positions of one node are one element.
-        if (p < TBH) {
-            if (p > 0 && sid[p] != kNone && sid[p] == sid[p - 1]) smerge(lp, uint32_t(SR + p), uint32_t(SR + p - 1));
-        } else {
-            const int k = p - TBH + 1;   // staged bottom index, column k - 1
-            if (sid[TBH + k] != kNone && sid[TBH + k] == sid[TBH + k - 1])
-                smerge(lp, uint32_t(SD + k), uint32_t(SD + k - 1));
-            if (p == TBH && sid[TBH + TBW + 1] != kNone && sid[TBH + TBW + 1] == sid[TBH + TBW])
-                smerge(lp, uint32_t(SD + TBW + 1), uint32_t(SD + TBW));
+        for (int p = threadIdx.x; p < K2_NP; p += K2_NT) {
+            if (p < TBH) {
+                if (p > 0 && sid[p] != kNone && sid[p] == sid[p - 1]) smerge(lp, uint32_t(SR + p), uint32_t(SR + p - 1));
+            } else {
+                const int k = p - TBH + 1;   // staged bottom index, column k - 1
+                if (sid[TBH + k] != kNone && sid[TBH + k] == sid[TBH + k - 1])
+                    smerge(lp, uint32_t(SD + k), uint32_t(SD + k - 1));
+                if (p == TBH && sid[TBH + TBW + 1] != kNone && sid[TBH + TBW + 1] == sid[TBH + TBW])
+                    smerge(lp, uint32_t(SD + TBW + 1), uint32_t(SD + TBW));
+            }
         }
         __syncthreads();
         auto pair = [&](uint32_t ja, uint32_t nA, uint32_t le, uint32_t nB) {
@@ -625,12 +651,14 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
             if (slot < uint32_t(kGQ2)) gq[slot] = make_uint2(nA, nB);
             else gunion2d(im, w, nA, nB);
         };
-        if (p < TBH) {
-            // Right border: neighbours in the tile to the right, same tile row.
-            const int r = p;
-            if (A) {
-                const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
-                uint32_t lastB = kNone;   // a node already paired with this one needs no second pair
+        for (int p = threadIdx.x; p < K2_NP; p += K2_NT) {
+            const uint32_t A = own[p];
+            if (!A) continue;
+            const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
+            uint32_t lastB = kNone;   // a node already paired with this one needs no second pair
+            if (p < TBH) {
+                // Right border: neighbours in the tile to the right, same tile row.
+                const int r = p;
 #pragma unroll
                 for (int d = -1; d <= 1; ++d) {
                     const int rr = r + d;
@@ -645,13 +673,9 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
                         lastB = nB;
                     }
                 }
-            }
-        } else {
-            // Bottom border: neighbours in the tile row below (including the diagonal tiles).
-            const int c = p - TBH;
-            if (A) {
-                const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
-                uint32_t lastB = kNone;
+            } else {
+                // Bottom border: neighbours in the tile row below (including the diagonal tiles).
+                const int c = p - TBH;
 #pragma unroll
                 for (int d = -1; d <= 1; ++d) {
                     const int k = c + d + 1;   // staged bottom index
@@ -726,22 +750,41 @@ __global__ void __launch_bounds__(K3_NT, 8) k_tile_write_2d(ImgList2D L, Work w)
 
     const int tid = threadIdx.x, lane = tid & 31;
     const uint16_t *lab = reinterpret_cast<const uint16_t *>(w.lab);
+    // Block entries and the root bitmap (first pixels of the components that stayed roots through
+    // the merge) were final before this grid's predecessor (segment scan and node flatten) started:
+    // that grid waits for the merge to complete before it lets this one launch.  So they are read
+    // before the wait (through L2), and only the segment prefixes, which the scan writes, after it.
+    // With a fixed tile order (no work queue) the CTA loads the next tile's entries, bitmap and
+    // node count into registers while it writes the current tile's labels.
+    static_assert(NBLK / 8 == 2 * K3_NT && RBWORDS == 2 * K3_NT, "two prefetched words per thread");
+    uint4 nL[2];
+    uint32_t nR[2], nNb = 0;
+    auto fetch = [&](int64_t t) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            nL[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + tid + i * K3_NT);
+            nR[i] = __ldcg(w.rbits + t * RBWORDS + tid + i * K3_NT);
+        }
+        nNb = __ldcg(w.nb + t);
+    };
+    const bool fixed_order = w.queue == nullptr;
     ItemLoop loop{w.queue ? w.queue + 4 : nullptr, w.n_tiles};
-    for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
+    int64_t t = loop.first(&qslot);
+    if (t < w.n_tiles) fetch(t);
+    for (bool first = true; t < w.n_tiles; t = loop.next(t, &qslot), first = false) {
+        if (!fixed_order && !first) fetch(t);   // a work queue gives the next tile only now
         const Img2D im = L.get(t);
         const int64_t lt = t - im.tile_base;
         const int ty = int(lt / im.tiles_x), tx = int(lt - int64_t(ty) * im.tiles_x);
         const int y0 = ty * TH, x0 = tx * TW;
         const int nrp = min(TH, im.rows - y0), ncp = min(TW, im.cols - x0);
-        // Block entries and the root bitmap (first pixels of the components that stayed roots
-        // through the merge) were final before this grid's predecessor (segment scan and node
-        // flatten) started: that grid waits for the merge to complete before it lets this one launch.  So they are
-        // read before the wait (through L2), and only the segment prefixes, which the scan writes,
-        // after it.
-        for (int i = tid; i < NBLK / 8; i += K3_NT)
-            reinterpret_cast<uint4 *>(Ls)[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + i);
-        for (int i = tid; i < RBWORDS; i += K3_NT) RB[i] = __ldcg(w.rbits + t * RBWORDS + i);
-        const uint32_t nb = __ldcg(w.nb + t);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            reinterpret_cast<uint4 *>(Ls)[tid + i * K3_NT] = nL[i];
+            RB[tid + i * K3_NT] = nR[i];
+        }
+        const uint32_t nb = nNb;
+        if (fixed_order && t + gridDim.x < w.n_tiles) fetch(t + gridDim.x);
         grid_dep_wait();   // segment prefixes from here on (returns at once after the first tile)
         const uint32_t base0 = w.segpref[im.seg_base];
         if (tid < TH && tid < nrp)
@@ -858,11 +901,13 @@ inline cudaError_t launch(const ImgList2D &L, const Work &w, int sms, bool persi
     k_tile_local_2d<<<grid(w.n_tiles, 7), K1_NT, 0, s>>>(L, wk);
     keep(cudaGetLastError());
     mark(1);
-    keep(launch_k(k_merge_2d, grid(w.n_tiles, 8), K2_NT, s, ov, L, wk));
+    keep(launch_k(k_merge_2d, grid(w.n_tiles, 28), K2_NT, s, ov, L, wk));
     mark(2);
     keep(launch_k(k_scan_flatten_2d, grid(int64_t(w.n_chunks) + w.n_tiles, 8), kScanThreads, s, ov, wk));
     mark(3);
-    keep(launch_k(k_tile_write_2d, grid(w.n_tiles, 8), K3_NT, s, ov, L, wk));
+    // The label writes run a fixed tile order over 8 CTAs per SM (they prefetch their next tile).
+    keep(launch_k(k_tile_write_2d, unsigned(std::max<int64_t>(1, std::min<int64_t>(w.n_tiles, int64_t(sms) * 8))),
+                  K3_NT, s, ov, L, wk));
     mark(4);
     return e;
 }

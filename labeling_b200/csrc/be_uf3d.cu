@@ -342,26 +342,6 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
             md[0] = make_uint4(mw[0], mw[1], mw[2], mw[3]);
             md[1] = make_uint4(mw[4], mw[5], mw[6], mw[7]);
         }
-        {
-            const uint32_t H00 = c[0] | c[1], H01 = c[2] | c[3], H10 = c[4] | c[5], H11 = c[6] | c[7];
-            uint32_t ss = S;
-            while (ss) {
-                const uint32_t s0 = __ffs(ss) - 1;
-                ss &= ss - 1;
-                const uint32_t from = ~0u << s0;
-                const uint32_t brk = ~hz & from;
-                const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
-                const uint32_t span = from & ((2u << e) - 1u);
-                int i, j;
-                uint32_t m;
-                if (H00 & span) { i = 0; j = 0; m = H00 & span; }
-                else if (H01 & span) { i = 0; j = 1; m = H01 & span; }
-                else if (H10 & span) { i = 1; j = 0; m = H10 & span; }
-                else { i = 1; j = 1; m = H11 & span; }
-                const uint32_t x = rowb + s0;
-                P[sw3(x)] = (slot3(b0, i, b1, j, __ffs(m) - 1) << 12) | x;
-            }
-        }
         __syncthreads();
 
         // Phase B: links to the four preceding rows (d0-1 with d1-1 / d1 / d1+1, and d0 with
@@ -410,12 +390,15 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
         auto start_of = [&](uint32_t b) -> uint32_t {
             return (b & ~31u) + hibit3(WS[b >> 5] & ((2u << (b & 31u)) - 1u));
         };
-        // Forest: a run takes its first link into the preceding layer (d0 - 1, whose slots are all
-        // smaller than this row's) as its parent, by a plain store of the parent's entry (its own
-        // root entry, or already its own parent's: an ancestor either way).  These links leave the
-        // queue.  Links within the same layer (d1 - 1) may go to larger slots and stay unions.
+        // Every run of this row gets its entry.  A run with a link into the preceding layer (d0 - 1,
+        // whose slots are all smaller than this row's) takes the first one as its parent by a plain
+        // store; the entry holds key 0, the smallest value, so no atomicMin of a union changes it and
+        // unions walk on to the parent (only a root's key is ever compared).  These links leave the
+        // queue.  Links within the same layer (d1 - 1) may go to larger slots and stay unions.  Any
+        // other run is a root for now: (slot << 12) | itself, the slot being that of its first voxel.
         // (Pointer jumping over the forest before the unions was measured slower.)
         {
+            const uint32_t H00 = c[0] | c[1], H01 = c[2] | c[3], H10 = c[4] | c[5], H11 = c[6] | c[7];
             uint32_t ss = S;
             while (ss) {
                 const uint32_t s0 = __ffs(ss) - 1;
@@ -423,6 +406,7 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
                 const uint32_t brk = ~hz & (~0u << s0);
                 const uint32_t e = brk ? uint32_t(__ffs(brk) - 1) : 31u;
                 const uint32_t span = (~0u << s0) & (0xFFFFFFFFu >> (31u - e));
+                const uint32_t x = rowb + s0;
                 bool found = false;
 #pragma unroll
                 for (int nr = 0; nr < 3; ++nr) {
@@ -442,7 +426,16 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
                         tgt = ubase + k + 1;
                         LE[nr] &= ~bit;
                     }
-                    P[sw3(rowb + s0)] = P[sw3(start_of(tgt))];
+                    P[sw3(x)] = start_of(tgt);   // key 0
+                }
+                if (!found) {
+                    int i, j;
+                    uint32_t m;
+                    if (H00 & span) { i = 0; j = 0; m = H00 & span; }
+                    else if (H01 & span) { i = 0; j = 1; m = H01 & span; }
+                    else if (H10 & span) { i = 1; j = 0; m = H10 & span; }
+                    else { i = 1; j = 1; m = H11 & span; }
+                    P[sw3(x)] = (slot3(b0, i, b1, j, __ffs(m) - 1) << 12) | x;
                 }
             }
         }
