@@ -203,7 +203,9 @@ cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persist
     mark(3);
     keep(launch_k(k_segscan, unsigned(std::max(w.n_chunks, 1)), kScanThreads, s, ov, wk));
     mark(4);
-    keep(launch_k(k_tile_write_3d, grid(w.n_tiles, 2), kT3Threads, s, ov, L, wk));
+    // The label writes run a fixed tile order over 5 CTAs per SM (they prefetch their next tile).
+    keep(launch_k(k_tile_write_3d, unsigned(std::max<int64_t>(1, std::min<int64_t>(w.n_tiles, int64_t(sms) * 5))),
+                  kT3Threads, s, ov, L, wk));
     mark(5);
     return e;
 }

@@ -9,7 +9,7 @@ constexpr int NPERIM = 2 * (TBW + TBH);            // border positions per tile
 constexpr int MAXB = NPERIM;                       // nodes per tile
 constexpr int WPR = TBW / 32;                      // 32-block words per block row
 constexpr int K1_NT = TBH * WPR;                   // one thread per (block row, word) = NBLK / 32
-constexpr int MQCAP = 1024;                        // union-queue capacity (more merge in place)
+constexpr int MQCAP = 608;                         // union-queue capacity (more take further rounds)
 constexpr uint32_t kPass = 0xFFFFu;                // "no run start" in the carry scan
 
 static_assert(NBLK <= 4096, "tile-local block index must fit 12 bits");
@@ -144,7 +144,7 @@ __device__ __forceinline__ void eunion(uint32_t *P, uint32_t a, uint32_t b)
 // operations; only runs enter the union-find, and only links between runs that no earlier link
 // already joins are merged.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(K1_NT, 7) k_tile_local_2d(ImgList2D L, Work w)
+__global__ void __launch_bounds__(K1_NT, 8) k_tile_local_2d(ImgList2D L, Work w)
 {
     grid_dep_release();   // the merge launch may take free SMs during this grid's last wave
     if (blockIdx.x == 0 && threadIdx.x == 0) {   // a new epoch for the segment scan of this run
@@ -156,8 +156,9 @@ __global__ void __launch_bounds__(K1_NT, 7) k_tile_local_2d(ImgList2D L, Work w)
     __shared__ uint32_t WBL[NBLK / 32], WBR[NBLK / 32], WHC[NBLK / 32], WS[NBLK / 32], WCS[NBLK / 32];
     __shared__ uint32_t RB[TH][TW / 32];
     __shared__ uint32_t BF[NBLK / 32];
-    __shared__ uint32_t BP[NBLK / 32];
     __shared__ uint32_t MQ[MQCAP];          // union queue: (block_a << 16) | block_b
+    static_assert(MQCAP >= NBLK / 32, "the node numbering reuses the queue's memory");
+    uint32_t *const BP = MQ;                // node numbering per 32 blocks (after the unions)
     __shared__ uint32_t mqn;
     __shared__ uint32_t tmp[K1_NT / 32 + 1];
     __shared__ uint32_t qslot;
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(K1_NT, 7) k_tile_local_2d(ImgList2D L, Work w)
         }
         // The remaining links are unions.  The queue holds the two blocks of each link; their run
         // starts are looked up by the merging lanes, which share that work evenly.  Links past the
-        // queue's capacity are merged in place by their own thread once every entry is written.
+        // queue's capacity go in in later rounds.
         const uint32_t n = __popc(Nm) + __popc(NWm) + __popc(NEm);
         const uint32_t pos0 = warp_reserve(&mqn, n);
         auto each_link = [&](auto &&f) {
@@ -395,18 +396,25 @@ __global__ void __launch_bounds__(K1_NT, 7) k_tile_local_2d(ImgList2D L, Work w)
                 if (pos < uint32_t(MQCAP)) MQ[pos] = (a << 16) | b;
             });
         __syncthreads();
+        // Rounds of the queue: the links with positions [base, base + MQCAP) go in, and each thread
+        // takes a contiguous run of them: neighbouring links, mostly of the same rows, are merged
+        // one after another by one thread instead of racing on the same roots.
         {
-            const uint32_t nq = min(mqn, uint32_t(MQCAP));
-            // Each thread takes a contiguous run of the queue: neighbouring links, mostly of the same
-            // rows, are merged one after another by one thread instead of racing on the same roots.
-            const uint32_t per = (nq + K1_NT - 1) / K1_NT, lo = min(nq, uint32_t(tid) * per), hi = min(nq, lo + per);
-            for (uint32_t i = lo; i < hi; ++i) eunion(P, start_of(MQ[i] >> 16), start_of(MQ[i] & 0xFFFFu));
-            if (pos0 + n > uint32_t(MQCAP))
-                each_link([&](uint32_t pos, uint32_t a, uint32_t b) {
-                    if (pos >= uint32_t(MQCAP)) eunion(P, start_of(a), start_of(b));
-                });
+            const uint32_t total = mqn;
+            for (uint32_t base = 0; base < total; base += MQCAP) {
+                if (base) {
+                    if (pos0 + n > base && pos0 < base + MQCAP)
+                        each_link([&](uint32_t pos, uint32_t a, uint32_t b) {
+                            if (pos >= base && pos < base + MQCAP) MQ[pos - base] = (a << 16) | b;
+                        });
+                    __syncthreads();
+                }
+                const uint32_t nq = min(total - base, uint32_t(MQCAP));
+                const uint32_t per = (nq + K1_NT - 1) / K1_NT, lo = min(nq, uint32_t(tid) * per), hi = min(nq, lo + per);
+                for (uint32_t i = lo; i < hi; ++i) eunion(P, start_of(MQ[i] >> 16), start_of(MQ[i] & 0xFFFFu));
+                __syncthreads();
+            }
         }
-        __syncthreads();
 
         // Phase C: every run start of this word, and every entry on its path, points straight at
         // its root (a read-only walk, then the root's entry stored along the path: every writer
@@ -898,7 +906,7 @@ inline cudaError_t launch(const ImgList2D &L, const Work &w, int sms, bool persi
         if (e == cudaSuccess) e = r;
     };
     mark(0);
-    k_tile_local_2d<<<grid(w.n_tiles, 7), K1_NT, 0, s>>>(L, wk);
+    k_tile_local_2d<<<grid(w.n_tiles, 8), K1_NT, 0, s>>>(L, wk);
     keep(cudaGetLastError());
     mark(1);
     keep(launch_k(k_merge_2d, grid(w.n_tiles, 28), K2_NT, s, ov, L, wk));

@@ -441,42 +441,46 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
         }
         __syncthreads();
         // The remaining links are unions, queued and merged by every lane, one neighbour row per
-        // round (the queue then holds a round's links; fewer rounds overflowed it and left the
-        // overflow to the warps that queued last).
+        // round; a round whose links overflow the queue takes further passes through it (the links
+        // with positions [base, base + MQ1) each), so the overflow is shared by every lane too.
 #pragma unroll
         for (int round = 0; round < 4; ++round) {
-            const int nr0 = round, nr1 = round + 1;
-            uint32_t n = 0;
-#pragma unroll
-            for (int nr = 0; nr < 4; ++nr)
-                if (nr >= nr0 && nr < nr1) n += __popc(LN[nr]) + __popc(LW[nr]) + __popc(LE[nr]);
-            uint32_t pos = warp_reserve(&mqn[round], n);
-            auto push = [&](uint32_t a, uint32_t b) {
-                if (pos < uint32_t(MQ1)) MQ[pos] = (a << 16) | b;
-                else eunion3(P, start_of(a), start_of(b));   // queue full: merge in place
-                ++pos;
-            };
-#pragma unroll
-            for (int nr = 0; nr < 4; ++nr) {
-                if (nr < nr0 || nr >= nr1) continue;
-                const uint32_t ubase = uint32_t(UR[nr]) * TB2;
-                uint32_t todo = LN[nr] | LW[nr] | LE[nr];
+            const uint32_t n = __popc(LN[round]) + __popc(LW[round]) + __popc(LE[round]);
+            const uint32_t pos0 = warp_reserve(&mqn[round], n);
+            const uint32_t ubase = uint32_t(UR[round]) * TB2;
+            auto each_link = [&](auto &&fn) {
+                uint32_t pos = pos0;
+                uint32_t todo = LN[round] | LW[round] | LE[round];
                 while (todo) {
                     const uint32_t k = __ffs(todo) - 1;
                     todo &= todo - 1;
                     const uint32_t bit = 1u << k;
                     const uint32_t a = rowb + k;
-                    if (LN[nr] & bit) push(a, ubase + k);
-                    if (LW[nr] & bit) push(a, ubase + k - 1);
-                    if (LE[nr] & bit) push(a, ubase + k + 1);
+                    if (LN[round] & bit) fn(pos++, a, ubase + k);
+                    if (LW[round] & bit) fn(pos++, a, ubase + k - 1);
+                    if (LE[round] & bit) fn(pos++, a, ubase + k + 1);
                 }
+            };
+            if (pos0 < uint32_t(MQ1))
+                each_link([&](uint32_t pos, uint32_t a, uint32_t b) {
+                    if (pos < uint32_t(MQ1)) MQ[pos] = (a << 16) | b;
+                });
+            __syncthreads();
+            const uint32_t total = mqn[round];
+            for (uint32_t base = 0; base < total; base += MQ1) {
+                if (base) {
+                    if (pos0 + n > base && pos0 < base + MQ1)
+                        each_link([&](uint32_t pos, uint32_t a, uint32_t b) {
+                            if (pos >= base && pos < base + MQ1) MQ[pos - base] = (a << 16) | b;
+                        });
+                    __syncthreads();
+                }
+                const uint32_t nq = min(total - base, uint32_t(MQ1));
+                // Contiguous runs of the queue per thread, as in 2D.
+                const uint32_t per = (nq + NT1 - 1) / NT1, lo = min(nq, uint32_t(tid) * per), hi = min(nq, lo + per);
+                for (uint32_t q = lo; q < hi; ++q) eunion3(P, start_of(MQ[q] >> 16), start_of(MQ[q] & 0xFFFFu));
+                __syncthreads();
             }
-            __syncthreads();
-            const uint32_t nq = min(mqn[round], uint32_t(MQ1));
-            // Contiguous runs of the queue per thread, as in 2D.
-            const uint32_t per = (nq + NT1 - 1) / NT1, lo = min(nq, uint32_t(tid) * per), hi = min(nq, lo + per);
-            for (uint32_t q = lo; q < hi; ++q) eunion3(P, start_of(MQ[q] >> 16), start_of(MQ[q] & 0xFFFFu));
-            __syncthreads();
         }
 
         // Phase C: every run start of this row, and every entry on its path, points straight at its
@@ -546,13 +550,28 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
             const uint32_t st = hibit3(WS[row] & ((2u << k) - 1u));
             return slot_block(P[sw3((row << 5) + st)] >> 12);
         };
-        for (int p = tid; p < NPERIM; p += NT1) {
+        // Each border position's root block and face bits, kept in registers for the entries below
+        // ((root << 4) | face bits, 16 bits each; 0 stands for an empty position -- a root block 0
+        // with no face voxel gives entry 0 as well).
+        constexpr int KP = NPERIM / NT1;
+        static_assert(NPERIM % NT1 == 0, "border positions per thread");
+        uint32_t pc[(KP + 1) / 2];
+#pragma unroll
+        for (int k = 0; k < KP; ++k) {
+            const int p = tid + k * NT1;
             int f, pb0, pb1, pb2;
-            if (!perim_pos3(p, g, f, pb0, pb1, pb2)) continue;
-            const int b = blk(pb0, pb1, pb2);
-            if (!M[b]) continue;
-            const uint32_t rb = root_block(b);
-            atomicOr(&BF[rb >> 5], 1u << (rb & 31));
+            uint32_t c = 0;
+            if (perim_pos3(p, g, f, pb0, pb1, pb2)) {
+                const int b = blk(pb0, pb1, pb2);
+                const uint32_t m = M[b];
+                if (m) {
+                    const uint32_t rb = root_block(b);
+                    atomicOr(&BF[rb >> 5], 1u << (rb & 31));
+                    c = (rb << 4) | face_bits(m, f);
+                }
+            }
+            if (k & 1) pc[k >> 1] |= c << 16;
+            else pc[k >> 1] = c;
         }
         __syncthreads();
         uint32_t nb;
@@ -581,19 +600,16 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
                 ++j;
             }
         }
-        for (int p = tid; p < NPERIM; p += NT1) {
-            int f, pb0, pb1, pb2;
+#pragma unroll
+        for (int k = 0; k < KP; ++k) {
+            const uint32_t c = (pc[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
             uint16_t ent = 0;
-            if (perim_pos3(p, g, f, pb0, pb1, pb2)) {
-                const int b = blk(pb0, pb1, pb2);
-                const uint32_t m = M[b];
-                if (m) {
-                    const uint32_t rb = root_block(b);
-                    const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
-                    ent = uint16_t((j << 4) | face_bits(m, f));
-                }
+            if (c) {
+                const uint32_t rb = c >> 4;
+                const uint32_t j = BP[rb >> 5] + __popc(BF[rb >> 5] & ((1u << (rb & 31)) - 1u));
+                ent = uint16_t((j << 4) | (c & 15u));
             }
-            w.perim[t * NPERIM + p] = ent;
+            w.perim[t * NPERIM + tid + k * NT1] = ent;
         }
         if (tid == 0) w.nb[t] = nb;
         __syncthreads();
@@ -623,7 +639,7 @@ __device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
 // goes on to the global union-find (from a shared queue, once the tile's pairs are all seen); a
 // dense volume that crosses a face with one component in hundreds of blocks costs a handful of
 // global unions.
-constexpr int kGQ3 = 1024;   // queued global unions per tile (more are done at once)
+constexpr int kGQ3 = 256;    // queued global unions per tile (more are done at once)
 constexpr int PF0 = (TB1 + 2) * (TB2 + 2);   // staged entries across the +d0 face
 constexpr int PF1 = (TB0 + 2) * (TB2 + 2);   // +d1
 constexpr int PF2 = (TB0 + 2) * (TB1 + 2);   // +d2
@@ -713,7 +729,7 @@ __device__ __forceinline__ bool staged_pos(int e, int &iu, int &iv)
     return true;
 }
 
-__global__ void __launch_bounds__(kT3MergeThreads, 4) k_merge_3d(ImgList3D L, Work w)
+__global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Work w)
 {
     grid_dep_wait();
     grid_dep_release();
@@ -939,18 +955,30 @@ __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
 
     const int tid = threadIdx.x;
     const uint32_t *lab = reinterpret_cast<const uint32_t *>(w.lab);
+    // Block entries and the post-merge node state were final before this grid's predecessor (the
+    // segment scan) started: that grid waits for the post-merge pass to complete before it lets
+    // this one launch.  So the root bitmap is built before the wait (reads through L2); only the
+    // segment prefixes, which the scan writes, come after it.  With a fixed tile order (no work
+    // queue) the CTA loads its next tile's block entries into registers while it writes the
+    // current tile's labels.
+    static_assert(NBLK / 4 == 4 * NT, "four prefetched words per thread");
+    uint4 nL[4];
+    auto fetch = [&](int64_t t) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) nL[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + tid + i * NT);
+    };
+    const bool fixed_order = w.queue == nullptr;
     ItemLoop loop{w.queue ? w.queue + 4 : nullptr, w.n_tiles};
-    for (int64_t t = loop.first(&qslot); t < w.n_tiles; t = loop.next(t, &qslot)) {
+    int64_t t = loop.first(&qslot);
+    if (t < w.n_tiles) fetch(t);
+    for (bool first = true; t < w.n_tiles; t = loop.next(t, &qslot), first = false) {
+        if (!fixed_order && !first) fetch(t);   // a work queue gives the next tile only now
         const Img3D im = L.get(t);
         const TileGeo g = tile_geo(im, t);
         const int64_t rs0 = int64_t(im.d1) * im.d2;
-
-        // Block entries and the post-merge node state were final before this grid's predecessor
-        // (the segment scan) started: that grid waits for the post-merge pass to complete before it
-        // lets this one launch.  So the root bitmap is built before the wait (reads through L2);
-        // only the segment prefixes, which the scan writes, come after it.
-        for (int i = tid; i < NBLK / 4; i += NT)
-            reinterpret_cast<uint4 *>(Ls)[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + i);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) reinterpret_cast<uint4 *>(Ls)[tid + i * NT] = nL[i];
+        if (fixed_order && t + gridDim.x < w.n_tiles) fetch(t + gridDim.x);
         for (int i = tid; i < TX * TY * RBW; i += NT) RB[i] = 0;
         __syncthreads();
 
