@@ -44,7 +44,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 STAGES_2D = ["k_tile_local_2d", "k_merge_2d", "k_scan_flatten_2d", "k_tile_write_2d"]
-STAGES_3D = ["k_tile_local_3d", "k_merge_3d", "k_post_3d", "k_segscan", "k_tile_write_3d"]
+STAGES_3D = ["k_tile_local_3d", "k_merge_3d", "k_scan_flatten_3d", "k_tile_write_3d"]
 # Algorithmic bytes per pixel of each launch (what the launch must move at minimum):
 # tile_local reads the image (1 B), tile_write writes the labels (4 B); the others move only
 # per-tile / per-segment metadata and have no per-pixel algorithmic traffic.

@@ -46,7 +46,7 @@ Geometry geometry_3d()
 {
     Geometry g;
     g.lab_bytes_per_tile = size_t(T3_NBLK) * sizeof(uint32_t);
-    g.rbits_bytes_per_tile = 0;
+    g.rbits_bytes_per_tile = size_t(2 * T3_TB0) * (2 * T3_TB1) * (2 * T3_TB2 / 32) * sizeof(uint32_t);
     g.nperim = T3_NPERIM;
     g.maxb = T3_MAXB;
     return g;
@@ -71,8 +71,6 @@ size_t layout_work(const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_img
     t.nb = reinterpret_cast<uint32_t *>(take(size_t(n_tiles) * sizeof(uint32_t)));
     t.gp = reinterpret_cast<uint32_t *>(take(nodes * sizeof(uint32_t)));
     t.nkey = reinterpret_cast<uint32_t *>(take(nodes * sizeof(uint32_t)));
-    t.grank = reinterpret_cast<uint32_t *>(take(nodes * sizeof(uint32_t)));
-    t.nlrank = reinterpret_cast<uint16_t *>(take(nodes * sizeof(uint16_t)));
     t.nroot = reinterpret_cast<uint16_t *>(take(nodes * sizeof(uint16_t)));
     t.segcnt = reinterpret_cast<uint8_t *>(take(align_up(size_t(n_segs), 16) + 16));
     t.segpref = reinterpret_cast<uint32_t *>(take((size_t(n_segs) + 1) * sizeof(uint32_t)));
@@ -199,14 +197,12 @@ cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persist
     mark(1);
     keep(launch_k(k_merge_3d, grid(w.n_tiles, 8), kT3MergeThreads, s, ov, L, wk));
     mark(2);
-    keep(launch_k(k_post_3d, grid(w.n_tiles + w.n_chunks, 12), kPostThreads, s, ov, L, wk));
+    keep(launch_k(k_scan_flatten_3d, grid(int64_t(w.n_chunks) + w.n_tiles, 8), kScanThreads, s, ov, wk));
     mark(3);
-    keep(launch_k(k_segscan, unsigned(std::max(w.n_chunks, 1)), kScanThreads, s, ov, wk));
-    mark(4);
     // The label writes run a fixed tile order over 5 CTAs per SM (they prefetch their next tile).
     keep(launch_k(k_tile_write_3d, unsigned(std::max<int64_t>(1, std::min<int64_t>(w.n_tiles, int64_t(sms) * 5))),
                   kT3Threads, s, ov, L, wk));
-    mark(5);
+    mark(4);
     return e;
 }
 
@@ -400,7 +396,7 @@ int be_label3d(be_ctx *c, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2,
         cudaMemsetAsync(c->ws3d.w.err, 0, 16 * sizeof(uint32_t), s);
 #endif
         e = launch_uf3d(L, c->ws3d.w, c->sms, false, s, c->timing ? c->stage_ev : nullptr);
-        c->timed_stages = c->timing ? kStages : 0;
+        c->timed_stages = c->timing ? kStages3D : 0;
         if (e != cudaSuccess) return cuda_error(c, e, "be_label3d launch");
     }
     if (rc) return rc;

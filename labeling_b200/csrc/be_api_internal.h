@@ -70,8 +70,9 @@ void fill_img2d(Img2D &im, const uint8_t *in, int64_t in_pitch, int32_t rows, in
                 int shape = 0);
 void fill_img3d(Img3D &im, const uint8_t *in, int32_t d0, int32_t d1, int32_t d2, int thr,
                 int32_t *out, int64_t tile_base, int64_t seg_base, int index);
-constexpr int kStages = 5;     // launches of the 3D union-find pipeline (the most of any form)
+constexpr int kStages = 5;     // stage events a context keeps (at least the launches of a pipeline)
 constexpr int kStages2D = 4;   // launches of the 2D union-find pipeline
+constexpr int kStages3D = 4;   // launches of the 3D union-find pipeline
 cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persistent, cudaStream_t s,
                         cudaEvent_t *ev = nullptr);
 

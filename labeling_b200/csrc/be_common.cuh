@@ -65,10 +65,9 @@ struct Work {
     uint32_t *nb;         // per tile: number of nodes
     uint32_t *gp;         // per node (tile * MAXB + j): union-find parent (global node id)
     uint32_t *nkey;       // per node: key of the node's root pixel
-    uint16_t *nlrank;     // per node: rank of the root among the tile's roots in its segment
     uint16_t *nroot;      // per node: tile-local block index of the node's root block
-    uint32_t *grank;      // per node that stays a root: rank among global roots in its segment
-    uint32_t *rbits;      // per tile: bitmap of the first pixels of the tile's components
+    uint32_t *rbits;      // per tile: bitmap of the first pixels (voxels) of the tile's components
+                          // that are still roots (the merge clears the ones it links)
     uint8_t *segcnt;      // per segment: number of component roots (uint8, word-padded)
     uint32_t *segpref;    // per segment + 1: exclusive prefix of segcnt over the launch
     uint32_t *chunksum;   // per scan chunk: sum of segcnt

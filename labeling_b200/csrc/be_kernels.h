@@ -22,14 +22,14 @@ namespace be {
 
 __global__ void k_tile_local_3d(ImgList3D L, Work w);
 __global__ void k_merge_3d(ImgList3D L, Work w);
-__global__ void k_post_3d(ImgList3D L, Work w);
+__global__ void k_scan_flatten_3d(Work w);
 __global__ void k_tile_write_3d(ImgList3D L, Work w);
 
 __global__ void k_segscan(Work w);
 __global__ void k_segscan_lb(Work w);
 __global__ void k_chunk_sums(Work w);
 
-constexpr int kPostThreads = 128;
+constexpr int kPostThreads = 128;   // k_chunk_sums
 constexpr int kT3Threads = 256;
 constexpr int kT3LocalThreads = T3_TB0 * T3_TB1;   // k_tile_local_3d: one thread per block row
 constexpr int kT3MergeThreads = 128;   // k_merge_3d: 8 tiles in flight per SM

@@ -1,6 +1,6 @@
 // be_scan.cu -- exclusive scan of the per-segment root counts: k_segscan is the second half of
-// the two-launch scan (the chunk sums run inside k_post_3d, or k_chunk_sums), k_segscan_lb the
-// single-pass form of the 2D pipeline.
+// the two-launch scan of the iterative forms (the chunk sums run in k_chunk_sums), k_segscan_lb
+// the single-pass form the union-find pipelines fuse with their node flatten.
 #include "be_kernels.h"
 #include "be_scan.cuh"
 

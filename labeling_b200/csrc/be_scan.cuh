@@ -127,4 +127,21 @@ __device__ __forceinline__ void segscan_lb_chunk(Work &w, uint32_t *tmp, uint32_
     if (c == w.n_chunks - 1 && threadIdx.x == 0) w.segpref[w.n_segs] = sh_excl + ctot;
 }
 
+// Points every linked node of tile t straight at its global root: all unions are done, so every
+// writer stores the same final root and any interleaving is safe.  Called by a whole CTA.
+__device__ __forceinline__ void flatten_tile_nodes(Work &w, int64_t t, int maxb)
+{
+    const uint32_t nb = w.nb[t];
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        const uint32_t node = uint32_t(t * maxb + j);
+        if (w.gp[node] == node) continue;
+        const uint32_t root = gfind_ro(w.gp, node);
+        for (uint32_t y = node; y != root;) {
+            const uint32_t ny = w.gp[y];
+            w.gp[y] = root;
+            y = ny;
+        }
+    }
+}
+
 }  // namespace be

@@ -726,18 +726,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_flatten_2d(Work w)
             segscan_lb_chunk<kScanThreads>(w, tmp, sh);
             continue;
         }
-        const int64_t t = it - w.n_chunks;
-        const uint32_t nb = w.nb[t];
-        for (uint32_t j = threadIdx.x; j < nb; j += kScanThreads) {
-            const uint32_t node = uint32_t(t * MAXB + j);
-            if (w.gp[node] == node) continue;
-            const uint32_t root = gfind_ro(w.gp, node);
-            for (uint32_t y = node; y != root;) {
-                const uint32_t ny = w.gp[y];
-                w.gp[y] = root;
-                y = ny;
-            }
-        }
+        flatten_tile_nodes(w, it - w.n_chunks, MAXB);
     }
 }
 

@@ -2,16 +2,19 @@
 //
 // Replaces the reference's BLEQ3D_Init / BLEQ3D_Scan / BLEQ3D_Analyze / BLEQ3D_SetFinalLabels
 // (LabelingAlgs.cl:740-979) and their host loop (LabelingAlgs.cpp:1443-1536) with the same
-// five-launch structure as the 2D pipeline (be_uf2d.cu):
+// four-launch structure as the 2D pipeline (be_uf2d_impl.cuh):
 //
 //   k_tile_local_3d   one CTA per 16 x 32 x 64-voxel tile (8 x 16 x 32 blocks): 16-byte loads,
 //                     8-bit block masks, shared-memory union-find over the 13 preceding
 //                     neighbours, flatten, per-component first-voxel key (atomicMin), one uint32
-//                     per block, segment root counts, border components exported as nodes.
-//   k_merge_3d        global union-find over nodes across the +d0 / +d1 / +d2 tile faces.
-//   k_post_3d         ranks of surviving border roots + scan-chunk sums.
-//   k_segscan         exclusive scan of the segment counts (be_scan.cu).
-//   k_tile_write_3d   resolves canonical labels and writes int32 voxels with 16-byte stores.
+//                     per block, segment root counts, a per-tile bitmap of component first
+//                     voxels, border components exported as nodes.
+//   k_merge_3d        global union-find over nodes across the +d0 / +d1 / +d2 tile faces; a root
+//                     linked under another leaves its segment count and its tile's bitmap.
+//   k_scan_flatten_3d exclusive scan of the segment counts (single pass, look-back) and
+//                     flattening of the linked nodes, one launch.
+//   k_tile_write_3d   resolves canonical labels (segment prefix + rank in the bitmap row) and
+//                     writes int32 voxels with 16-byte stores.
 //
 // Volume layout is the reference's cv::Mat 3-D order [d0][d1][d2] with d2 fastest
 // (Read3DImage, main.cpp:191-203; kernel addressing x*h*d + y*d + z, LabelingAlgs.cl:974).
@@ -258,6 +261,10 @@ __device__ __forceinline__ void split16b(uint4 v, uint32_t K, bool hi, uint32_t 
 __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
 {
     grid_dep_release();   // the merge launch may take free SMs during this grid's last wave
+    if (blockIdx.x == 0 && threadIdx.x == 0) {   // a new epoch for the segment scan of this run
+        w.epoch[0] += 1u;
+        w.epoch[1] = 0u;
+    }
     __shared__ uint32_t P[NBLK];               // run starts: (slot << 12) | parent
     __shared__ __align__(16) uint8_t M[NBLK];  // block masks
     __shared__ uint32_t CW[8][NT1];            // class words of every row
@@ -535,7 +542,8 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
         }
         __syncthreads();   // root bitmap complete; every run start points at its root
 
-        // Phase D: segment counts and border nodes.
+        // Phase D: root bitmap and segment counts out, border nodes.
+        for (int i = tid; i < TX * TY * RBW; i += NT1) w.rbits[t * (TX * TY * RBW) + i] = RB[i];
         for (int r = tid; r < TX * TY; r += NT1) {
             const int X = r / TY, Y = r % TY;
             if (X >= g.nx || Y >= g.ny) continue;
@@ -589,13 +597,9 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
                 if (!GUARD(w, key < uint32_t(TX * TY * TZ) && j < uint32_t(MAXB), 102, (uint64_t(j) << 32) | key))
                     break;
                 const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
-                const uint32_t *row = &RB[(X * TY + Y) * RBW];
-                uint32_t rank = __popc(row[Z >> 5] & ((1u << (Z & 31)) - 1u));
-                for (int k = 0; k < (Z >> 5); ++k) rank += __popc(row[k]);
                 const int64_t node = t * MAXB + j;
                 w.nroot[node] = uint16_t(rb);
                 w.nkey[node] = uint32_t((int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.d2 + (g.z0 + Z));
-                w.nlrank[node] = uint16_t(rank);
                 w.gp[node] = uint32_t(node);
                 ++j;
             }
@@ -621,11 +625,35 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
 // ---------------------------------------------------------------------------------------------
 namespace {
 
+// Where the voxel with raster key `key` of image im sits: its tile, the root-bitmap word and bit of
+// it in that tile, and its segment.
+struct KeyPos {
+    int64_t tile, word, seg;
+    uint32_t bit;
+};
+__device__ __forceinline__ KeyPos key_pos(const Img3D &im, uint32_t key)
+{
+    // Keys index one volume (< 2^32 voxels): 32-bit division suffices.
+    const uint32_t row = key / uint32_t(im.d2), Z = key - row * uint32_t(im.d2);
+    const uint32_t X = row / uint32_t(im.d1), Y = row - X * uint32_t(im.d1);
+    const uint32_t q0 = X / TX, q1 = Y / TY, q2 = Z / TZ;
+    KeyPos kp;
+    kp.tile = im.tile_base + (int64_t(q0) * im.t1 + q1) * im.t2 + q2;
+    const uint32_t lx = X % TX, ly = Y % TY, lz = Z % TZ;
+    kp.word = kp.tile * (TX * TY * RBW) + int64_t((lx * TY + ly) * RBW + (lz >> 5));
+    kp.bit = lz & 31u;
+    kp.seg = im.seg_base + int64_t(row) * im.t2 + q2;
+    return kp;
+}
+
+// Union of two nodes of one volume; the root linked under the other leaves its segment's root
+// count and its tile's root bitmap.
 __device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
 {
     gunion_keyed(w.gp, w.nkey, a, b, [&](uint32_t key) {
-        const int64_t row = key / uint32_t(im.d2), z = key - row * im.d2;
-        dec_u8(w.segcnt, im.seg_base + row * im.t2 + z / TZ);
+        const KeyPos kp = key_pos(im, key);
+        dec_u8(w.segcnt, kp.seg);
+        atomicAnd(w.rbits + kp.word, ~(1u << kp.bit));
     });
 }
 
@@ -874,78 +902,29 @@ __global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Wo
 }
 
 // ---------------------------------------------------------------------------------------------
-// Post-merge ranks of surviving border roots, and scan-chunk sums.
+// Segment scan and node flatten, one launch: items below n_chunks scan a chunk of segment counts
+// (single pass, look-back); the others point every linked node of one tile straight at its global
+// root, so that the label writes find each root in one step.
 // ---------------------------------------------------------------------------------------------
-namespace {
-
-__device__ void post_tile_3d(const ImgList3D &L, Work &w, int64_t t)
-{
-    __shared__ uint32_t LB[TX * TY * RBW];   // keys of linked nodes
-    const Img3D im = L.get(t);
-    const TileGeo g = tile_geo(im, t);
-    const uint32_t nb = w.nb[t];
-    for (int i = threadIdx.x; i < TX * TY * RBW; i += blockDim.x) LB[i] = 0;
-    __syncthreads();
-    auto local = [&](uint32_t key, int &X, int &Y, int &Z) {
-        const uint32_t row = key / uint32_t(im.d2);
-        Z = int(key - row * uint32_t(im.d2)) - g.z0;
-        const uint32_t xg = row / uint32_t(im.d1);
-        Y = int(row - xg * uint32_t(im.d1)) - g.y0;
-        X = int(xg) - g.x0;
-    };
-    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
-        const int64_t node = t * MAXB + j;
-        if (w.gp[node] == uint32_t(node)) continue;
-        // All unions are done: point the node's whole path at its root, so that the label pass
-        // (and the other tiles' walks here) find it in one step.
-        {
-            const uint32_t root = gfind_ro(w.gp, uint32_t(node));
-            for (uint32_t y = uint32_t(node); y != root;) {
-                const uint32_t ny = w.gp[y];
-                w.gp[y] = root;
-                y = ny;
-            }
-        }
-        int X, Y, Z;
-        local(w.nkey[node], X, Y, Z);
-        if (GUARD(w, X >= 0 && X < TX && Y >= 0 && Y < TY && Z >= 0 && Z < TZ, 301, w.nkey[node]))
-            atomicOr(&LB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
-    }
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
-        const int64_t node = t * MAXB + j;
-        if (w.gp[node] != uint32_t(node)) continue;
-        int X, Y, Z;
-        local(w.nkey[node], X, Y, Z);
-        if (!GUARD(w, X >= 0 && X < TX && Y >= 0 && Y < TY && Z >= 0 && Z < TZ, 302, w.nkey[node])) continue;
-        const uint32_t *row = &LB[(X * TY + Y) * RBW];
-        uint32_t cnt = __popc(row[Z >> 5] & ((1u << (Z & 31)) - 1u));
-        for (int k = 0; k < (Z >> 5); ++k) cnt += __popc(row[k]);
-        w.grank[node] = w.nlrank[node] - cnt;
-    }
-    __syncthreads();
-}
-
-}  // namespace
-
-__global__ void __launch_bounds__(kPostThreads) k_post_3d(ImgList3D L, Work w)
+__global__ void __launch_bounds__(kScanThreads) k_scan_flatten_3d(Work w)
 {
     grid_dep_wait();
-    grid_dep_release();
-    __shared__ uint32_t tmp[kPostThreads / 32 + 1];
+    grid_dep_release();   // after the wait: the label-write launch relies on it
+    __shared__ uint32_t tmp[kScanThreads / 32 + 1];
+    __shared__ uint32_t sh[2];
     __shared__ uint32_t qslot;
-    const int64_t n = w.n_tiles + w.n_chunks;
+    const int64_t n = int64_t(w.n_chunks) + w.n_tiles;
     ItemLoop loop{w.queue ? w.queue + 2 : nullptr, n};
     for (int64_t it = loop.first(&qslot); it < n; it = loop.next(it, &qslot)) {
-        if (it < w.n_tiles) post_tile_3d(L, w, it);
-        else chunk_sum<kPostThreads>(w, it - w.n_tiles, tmp);
+        if (it < w.n_chunks) segscan_lb_chunk<kScanThreads>(w, tmp, sh);
+        else flatten_tile_nodes(w, it - w.n_chunks, MAXB);
     }
 }
 
 // ---------------------------------------------------------------------------------------------
 // Label resolve and write.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
+__global__ void __launch_bounds__(NT, 5) k_tile_write_3d(ImgList3D L, Work w)
 {
     __shared__ __align__(16) uint32_t Ls[NBLK];
     __shared__ uint32_t LT[NBLK];
@@ -955,17 +934,21 @@ __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
 
     const int tid = threadIdx.x;
     const uint32_t *lab = reinterpret_cast<const uint32_t *>(w.lab);
-    // Block entries and the post-merge node state were final before this grid's predecessor (the
-    // segment scan) started: that grid waits for the post-merge pass to complete before it lets
-    // this one launch.  So the root bitmap is built before the wait (reads through L2); only the
-    // segment prefixes, which the scan writes, come after it.  With a fixed tile order (no work
-    // queue) the CTA loads its next tile's block entries into registers while it writes the
+    // Block entries and root bitmaps were final before this grid's predecessor (the scan and
+    // flatten) started: that grid waits for the merge to complete before it lets this one launch.
+    // So both are read before the wait (through L2); the segment prefixes and the flattened node
+    // links, which the predecessor writes, come after it.  With a fixed tile order (no work queue)
+    // the CTA loads its next tile's block entries and bitmap into registers while it writes the
     // current tile's labels.
-    static_assert(NBLK / 4 == 4 * NT, "four prefetched words per thread");
+    static_assert(NBLK / 4 == 4 * NT && TX * TY * RBW == 4 * NT, "four prefetched words per thread");
     uint4 nL[4];
+    uint32_t nR[4];
     auto fetch = [&](int64_t t) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) nL[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + tid + i * NT);
+        for (int i = 0; i < 4; ++i) {
+            nL[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + tid + i * NT);
+            nR[i] = __ldcg(w.rbits + t * (TX * TY * RBW) + tid + i * NT);
+        }
     };
     const bool fixed_order = w.queue == nullptr;
     ItemLoop loop{w.queue ? w.queue + 4 : nullptr, w.n_tiles};
@@ -977,30 +960,12 @@ __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
         const TileGeo g = tile_geo(im, t);
         const int64_t rs0 = int64_t(im.d1) * im.d2;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) reinterpret_cast<uint4 *>(Ls)[tid + i * NT] = nL[i];
+        for (int i = 0; i < 4; ++i) {
+            reinterpret_cast<uint4 *>(Ls)[tid + i * NT] = nL[i];
+            RB[tid + i * NT] = nR[i];
+        }
         if (fixed_order && t + gridDim.x < w.n_tiles) fetch(t + gridDim.x);
-        for (int i = tid; i < TX * TY * RBW; i += NT) RB[i] = 0;
-        __syncthreads();
-
-        for (int b = tid; b < NBLK; b += NT) {
-            const uint32_t e = Ls[b];
-            if (!(e & ROOT_FLAG)) continue;
-            const uint32_t key = e & (ROOT_FLAG - 1);
-            const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
-            if (GUARD(w, key < uint32_t(TX * TY * TZ), 401, key))
-                atomicOr(&RB[(X * TY + Y) * RBW + (Z >> 5)], 1u << (Z & 31));
-        }
-        __syncthreads();
         const uint32_t nb = __ldcg(w.nb + t);
-        for (uint32_t j = tid; j < nb; j += NT) {
-            const int64_t node = t * MAXB + j;
-            if (__ldcg(w.gp + node) == uint32_t(node)) continue;
-            const uint32_t nr = __ldcg(w.nroot + node);
-            if (!GUARD(w, nr < NBLK && (Ls[nr % NBLK] & ROOT_FLAG), 402, node)) continue;
-            const uint32_t key = Ls[nr] & (ROOT_FLAG - 1);
-            const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
-            atomicAnd(&RB[(X * TY + Y) * RBW + (Z >> 5)], ~(1u << (Z & 31)));
-        }
         grid_dep_wait();   // segment prefixes from here on (returns at once after the first tile)
         const uint32_t base0 = w.segpref[im.seg_base];
         for (int r = tid; r < TX * TY; r += NT) {
@@ -1022,16 +987,19 @@ __global__ void __launch_bounds__(NT) k_tile_write_3d(ImgList3D L, Work w)
             LT[b] = 1u + segb[X * TY + Y] + rank;
         }
         __syncthreads();
+        // Border components linked under another tile's component: the label of that root, its
+        // segment's prefix plus its rank among the first voxels left in its row of its tile.
         for (uint32_t j = tid; j < nb; j += NT) {
             const int64_t node = t * MAXB + j;
-            if (w.gp[node] == uint32_t(node)) continue;
-            const uint32_t gn = gfind_ro(w.gp, uint32_t(node));
-            const uint32_t kg = w.nkey[gn];
-            const int64_t row = kg / uint32_t(im.d2), z = kg - row * im.d2;
-            const int64_t si = im.seg_base + row * im.t2 + z / TZ;
-            if (!GUARD(w, si >= 0 && si <= w.n_segs, 404, si)) continue;
-            const uint32_t sb = w.segpref[si] - base0;
-            LT[w.nroot[node]] = 1u + sb + w.grank[gn];
+            if (__ldcg(w.gp + node) == uint32_t(node)) continue;
+            const uint32_t gn = gfind_halve(w.gp, uint32_t(node));
+            const KeyPos kp = key_pos(im, __ldcg(w.nkey + gn));
+            if (!GUARD(w, kp.seg >= 0 && kp.seg < w.n_segs && kp.tile >= 0 && kp.tile < w.n_tiles, 404, kp.seg)) continue;
+            const uint32_t *rw = w.rbits + (kp.word & ~int64_t(RBW - 1));
+            uint32_t rank = __popc(__ldcg(rw + (kp.word & (RBW - 1))) & ((1u << kp.bit) - 1u));
+            for (int k = 0; k < int(kp.word & (RBW - 1)); ++k) rank += __popc(__ldcg(rw + k));
+            const uint32_t nr = __ldcg(w.nroot + node);
+            if (GUARD(w, nr < uint32_t(NBLK), 402, node)) LT[nr] = 1u + (w.segpref[kp.seg] - base0) + rank;
         }
         __syncthreads();
 
