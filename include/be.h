@@ -39,7 +39,8 @@ typedef enum be_status {
     BE_ERR_TIMEOUT = 5,        /* a bounded wait ran out (server / batch) */
     BE_ERR_BUSY = 6,           /* admission refused: not enough free device memory or slots */
     BE_ERR_CANCELLED = 7,      /* the request was cancelled before it completed */
-    BE_ERR_TOO_LARGE = 8       /* the image exceeds the fixed scratch of be_label2d_noalloc */
+    BE_ERR_TOO_LARGE = 8       /* the image exceeds the fixed scratch of be_label2d_noalloc, or one
+                                  launch holds more than 2^32 - 2 image rows (voxel rows) */
 } be_status;
 
 /* Merge algorithm. */

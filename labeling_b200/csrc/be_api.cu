@@ -49,6 +49,7 @@ Geometry geometry_3d()
     g.rbits_bytes_per_tile = size_t(2 * T3_TB0) * (2 * T3_TB1) * (2 * T3_TB2 / 32) * sizeof(uint32_t);
     g.nperim = T3_NPERIM;
     g.maxb = T3_MAXB;
+    g.links = true;
     return g;
 }
 
@@ -72,6 +73,7 @@ size_t layout_work(const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_img
     t.gp = reinterpret_cast<uint32_t *>(take(nodes * sizeof(uint32_t)));
     t.nkey = reinterpret_cast<uint32_t *>(take(nodes * sizeof(uint32_t)));
     t.nroot = reinterpret_cast<uint16_t *>(take(nodes * sizeof(uint16_t)));
+    t.nlink = g.links ? reinterpret_cast<uint2 *>(take(nodes * sizeof(uint2))) : nullptr;
     t.segcnt = reinterpret_cast<uint8_t *>(take(align_up(size_t(n_segs), 16) + 16));
     t.segpref = reinterpret_cast<uint32_t *>(take((size_t(n_segs) + 1) * sizeof(uint32_t)));
     t.chunksum = reinterpret_cast<uint32_t *>(take(size_t(std::max<int64_t>(n_chunks, 1)) * sizeof(uint32_t)));
@@ -97,6 +99,8 @@ cudaError_t reset_scan_state(const Work &w, cudaStream_t s)
 
 int Workspace::ensure(be_ctx *ctx, const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_imgs)
 {
+    // Node links name a segment in 32 bits.
+    if (n_segs >= int64_t(kNone)) return set_error(ctx, BE_ERR_TOO_LARGE, "more than 2^32 - 2 image rows in one launch");
     const size_t need = layout_work(g, n_tiles, n_segs, n_imgs, nullptr, nullptr);
     if (!base || need > bytes) {
         if (base) {
@@ -197,7 +201,7 @@ cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persist
     mark(1);
     keep(launch_k(k_merge_3d, grid(w.n_tiles, 8), kT3MergeThreads, s, ov, L, wk));
     mark(2);
-    keep(launch_k(k_scan_flatten_3d, grid(int64_t(w.n_chunks) + w.n_tiles, 8), kScanThreads, s, ov, wk));
+    keep(launch_k(k_scan_link_3d, grid(int64_t(w.n_chunks) + w.n_tiles, 8), kScanThreads, s, ov, L, wk));
     mark(3);
     // The label writes run a fixed tile order over 5 CTAs per SM (they prefetch their next tile).
     keep(launch_k(k_tile_write_3d, unsigned(std::max<int64_t>(1, std::min<int64_t>(w.n_tiles, int64_t(sms) * 5))),

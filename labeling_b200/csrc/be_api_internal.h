@@ -17,6 +17,7 @@ struct Geometry {
     size_t rbits_bytes_per_tile;
     int nperim;
     int maxb;
+    bool links = false;   // the pipeline resolves node links (Work::nlink) before its label writes
 };
 
 // 2D tile shapes (in 2x2 blocks); shape 0 is the default.

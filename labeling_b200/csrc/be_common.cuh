@@ -66,6 +66,9 @@ struct Work {
     uint32_t *gp;         // per node (tile * MAXB + j): union-find parent (global node id)
     uint32_t *nkey;       // per node: key of the node's root pixel
     uint16_t *nroot;      // per node: tile-local block index of the node's root block
+    uint2 *nlink;         // per node, after the merge: x = segment of its global root's first pixel
+                          // (kNone when the node is a root itself), y = (root block << 16) | rank
+                          // of that first pixel among the roots left in its segment
     uint32_t *rbits;      // per tile: bitmap of the first pixels (voxels) of the tile's components
                           // that are still roots (the merge clears the ones it links)
     uint8_t *segcnt;      // per segment: number of component roots (uint8, word-padded)
@@ -394,6 +397,28 @@ using ImgList3D = ImgList<Img3D>;
 // global access, so the overlap only hides launch and ramp-up time, never a dependency.
 __device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void grid_dep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Asynchronous global -> shared copies (cp.async, through L1): the data lands in shared memory
+// without passing through registers, so a CTA can fetch its next tile's small arrays while it
+// works on the current one.  cp_async_wait() waits for all of this thread's copies; a barrier
+// after it makes every thread's copies visible to the CTA.
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)   // L2 only
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Launches kernel k, with programmatic stream serialization when `overlap` is set.
 template <typename... P, typename... A>

@@ -22,7 +22,7 @@ namespace be {
 
 __global__ void k_tile_local_3d(ImgList3D L, Work w);
 __global__ void k_merge_3d(ImgList3D L, Work w);
-__global__ void k_scan_flatten_3d(Work w);
+__global__ void k_scan_link_3d(ImgList3D L, Work w);
 __global__ void k_tile_write_3d(ImgList3D L, Work w);
 
 __global__ void k_segscan(Work w);

@@ -1,8 +1,10 @@
-// be_scan.cuh -- the segment-count scan shared by the 2D and 3D pipelines.
+// be_scan.cuh -- the segment-count scan and the node-link pass shared by the 2D and 3D pipelines.
 //
-// Segment counts are uint8 (at most half a segment's pixels can start a component).  The scan
-// runs in two launches: k_post_* sums each chunk of kScanChunk counts (chunk_sum below) while it
-// ranks border roots, and k_segscan turns the counts into an exclusive uint32 prefix.
+// Segment counts are uint8 (at most half a segment's pixels can start a component).  The
+// union-find pipelines scan them in one launch (segscan_lb_chunk, a single-pass scan with a
+// decoupled look-back) beside the node pass (flatten_tile_nodes in 2D, link_tile_nodes in 3D);
+// the iterative forms use the two-launch scan of be_scan.cu (k_chunk_sums with chunk_sum below,
+// then k_segscan).
 #pragma once
 #include "be_common.cuh"
 
@@ -141,6 +143,33 @@ __device__ __forceinline__ void flatten_tile_nodes(Work &w, int64_t t, int maxb)
             w.gp[y] = root;
             y = ny;
         }
+    }
+}
+
+// As flatten_tile_nodes, and resolves each node's link for the label writes: nlink[node] =
+// (segment of the root's first pixel, (node's root block << 16) | rank of that pixel among the
+// roots left in its segment), or x = kNone for a node that is a root.  locate(key, &seg, &rank)
+// finds the segment and the rank of the pixel with raster key `key` from the root bitmaps, which
+// the merge has left final.  Called by a whole CTA.
+template <typename Locate>
+__device__ __forceinline__ void link_tile_nodes(Work &w, int64_t t, int maxb, Locate locate)
+{
+    const uint32_t nb = w.nb[t];
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        const uint32_t node = uint32_t(t * maxb + j);
+        uint2 link = make_uint2(kNone, 0u);
+        if (w.gp[node] != node) {
+            const uint32_t root = gfind_ro(w.gp, node);
+            for (uint32_t y = node; y != root;) {
+                const uint32_t ny = w.gp[y];
+                w.gp[y] = root;
+                y = ny;
+            }
+            uint32_t seg, rank;
+            locate(w.nkey[root], seg, rank);
+            link = make_uint2(seg, (uint32_t(w.nroot[node]) << 16) | rank);
+        }
+        w.nlink[node] = link;
     }
 }
 

@@ -668,6 +668,7 @@ __device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
 // dense volume that crosses a face with one component in hundreds of blocks costs a handful of
 // global unions.
 constexpr int kGQ3 = 256;    // queued global unions per tile (more are done at once)
+constexpr int kPL3 = 1152;   // listed face pairs per tile (more are checked where they are found)
 constexpr int PF0 = (TB1 + 2) * (TB2 + 2);   // staged entries across the +d0 face
 constexpr int PF1 = (TB0 + 2) * (TB2 + 2);   // +d1
 constexpr int PF2 = (TB0 + 2) * (TB1 + 2);   // +d2
@@ -767,7 +768,7 @@ __global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Wo
     __shared__ uint8_t nbf[NPF];          // its face bits
     __shared__ uint2 gq[kGQ3];
     __shared__ uint32_t nq;
-    __shared__ uint32_t pl[kT3MergeThreads * 9];   // one round's listed pairs: (node << 16) | staged
+    __shared__ uint32_t pl[kPL3];         // listed pairs: (node << 16) | staged position
     __shared__ uint32_t npl;
     __shared__ uint16_t own[NPLUS];       // this tile's + face entries (staged with the others)
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
@@ -775,7 +776,10 @@ __global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Wo
         const Img3D im = L.get(t);
         const TileGeo g = tile_geo(im, t);
         for (int i = threadIdx.x; i < MAXB + NPF; i += kT3MergeThreads) lp[i] = uint32_t(i);
-        if (threadIdx.x == 0) nq = 0;
+        if (threadIdx.x == 0) {
+            nq = 0;
+            npl = 0;
+        }
         for (int e = threadIdx.x; e < PF0; e += kT3MergeThreads) stage_face<0>(im, g, w, e, nbid, nbf);
         for (int e = threadIdx.x; e < PF1; e += kT3MergeThreads) stage_face<1>(im, g, w, e, nbid, nbf);
         for (int e = threadIdx.x; e < PF2; e += kT3MergeThreads) stage_face<2>(im, g, w, e, nbid, nbf);
@@ -824,10 +828,19 @@ __global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Wo
         for (int e = threadIdx.x; e < NPF; e += kT3MergeThreads)
             if (nbid[e] != kNone) sflatten(lp, uint32_t(MAXB + e));
         __syncthreads();
-        // Pairs: each round, the face positions of one CTA-width list their connected neighbours
-        // (a bit test each), then all lanes check the listed pairs; a pair whose two elements are
-        // already one local set is implied by pairs queued before it (smerge_joined).  The rest
-        // are unioned globally after the rounds.
+        // Pairs: every face position lists its connected neighbours (a bit test each) in one pass
+        // over the three faces, then all lanes check the listed pairs; a pair whose two elements are
+        // already one local set is implied by pairs queued before it (smerge_joined).  Pairs past
+        // the list's capacity are checked by the lane that finds them.  The rest are unioned
+        // globally at the end.
+        auto check_pair = [&](uint32_t ja2, uint32_t e) {
+            if (!smerge_joined(lp, ja2, uint32_t(MAXB) + e)) return;
+            const uint32_t nA = uint32_t(t * MAXB + ja2), id = nbid[e];
+            const uint32_t slot = atomicAdd(&nq, 1u);
+            if (slot < uint32_t(kGQ3)) gq[slot] = make_uint2(nA, id);
+            else gunion3d(im, w, nA, id);
+        };
+        const uint32_t nbt = w.nb[t];
         for (int base = 0; base < NPLUS; base += kT3MergeThreads) {
             const int p = base + int(threadIdx.x);
             int u = 0, v = 0, ebase = 0, pitch = 1;
@@ -843,7 +856,7 @@ __global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Wo
                 ebase = FaceAx<2>::EBASE; pitch = FaceAx<2>::PITCH;
             }
             if (p < NPLUS) A = own[p];
-            if (A && !GUARD(w, (A >> 4) < w.nb[t] && (A >> 4) < uint32_t(MAXB), 204, (uint64_t(t) << 16) | (A >> 4)))
+            if (A && !GUARD(w, (A >> 4) < nbt && (A >> 4) < uint32_t(MAXB), 204, (uint64_t(t) << 16) | (A >> 4)))
                 A = 0;
             const uint32_t fa = A & 15u, ja = A >> 4;
             uint32_t hit = 0;   // bit 3 * (da + 1) + (db + 1): connected neighbour
@@ -858,8 +871,6 @@ __global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Wo
                     }
                 }
             }
-            if (threadIdx.x == 0) npl = 0;
-            __syncthreads();
             // Neighbours whose staged positions already share a local parent are one local set
             // (mostly one node's patch across the face): the first of them stands for the others.
             uint32_t keep = 0;
@@ -879,20 +890,16 @@ __global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Wo
             while (keep) {
                 const int k = __ffs(keep) - 1;
                 keep &= keep - 1;
-                const int e = ebase + (u + k / 3) * pitch + (v + k % 3);
-                pl[pos++] = (ja << 16) | uint32_t(e);
+                const uint32_t e = uint32_t(ebase + (u + k / 3) * pitch + (v + k % 3));
+                if (pos < uint32_t(kPL3)) pl[pos] = (ja << 16) | e;
+                else check_pair(ja, e);
+                ++pos;
             }
-            __syncthreads();
-            const uint32_t n = npl;
-            for (uint32_t i = threadIdx.x; i < n; i += kT3MergeThreads) {
-                const uint32_t ja2 = pl[i] >> 16, e = pl[i] & 0xFFFFu;
-                if (!smerge_joined(lp, ja2, uint32_t(MAXB) + e)) continue;
-                const uint32_t nA = uint32_t(t * MAXB + ja2), id = nbid[e];
-                const uint32_t slot = atomicAdd(&nq, 1u);
-                if (slot < uint32_t(kGQ3)) gq[slot] = make_uint2(nA, id);
-                else gunion3d(im, w, nA, id);
-            }
-            __syncthreads();
+        }
+        __syncthreads();
+        {
+            const uint32_t n = min(npl, uint32_t(kPL3));
+            for (uint32_t i = threadIdx.x; i < n; i += kT3MergeThreads) check_pair(pl[i] >> 16, pl[i] & 0xFFFFu);
         }
         __syncthreads();
         const uint32_t nqt = min(nq, uint32_t(kGQ3));
@@ -902,11 +909,12 @@ __global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Wo
 }
 
 // ---------------------------------------------------------------------------------------------
-// Segment scan and node flatten, one launch: items below n_chunks scan a chunk of segment counts
-// (single pass, look-back); the others point every linked node of one tile straight at its global
-// root, so that the label writes find each root in one step.
+// Segment scan and node links, one launch: items below n_chunks scan a chunk of segment counts
+// (single pass, look-back); the others resolve the linked nodes of one tile (link_tile_nodes):
+// each is pointed straight at its global root, and the segment and in-segment rank of that root's
+// first voxel are stored with it.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kScanThreads) k_scan_flatten_3d(Work w)
+__global__ void __launch_bounds__(kScanThreads) k_scan_link_3d(ImgList3D L, Work w)
 {
     grid_dep_wait();
     grid_dep_release();   // after the wait: the label-write launch relies on it
@@ -916,39 +924,68 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_flatten_3d(Work w)
     const int64_t n = int64_t(w.n_chunks) + w.n_tiles;
     ItemLoop loop{w.queue ? w.queue + 2 : nullptr, n};
     for (int64_t it = loop.first(&qslot); it < n; it = loop.next(it, &qslot)) {
-        if (it < w.n_chunks) segscan_lb_chunk<kScanThreads>(w, tmp, sh);
-        else flatten_tile_nodes(w, it - w.n_chunks, MAXB);
+        if (it < w.n_chunks) {
+            segscan_lb_chunk<kScanThreads>(w, tmp, sh);
+            continue;
+        }
+        const int64_t t = it - w.n_chunks;
+        const Img3D im = L.get(t);
+        link_tile_nodes(w, t, MAXB, [&](uint32_t key, uint32_t &seg, uint32_t &rank) {
+            const KeyPos kp = key_pos(im, key);
+            const uint32_t *rw = w.rbits + (kp.word & ~int64_t(RBW - 1));
+            rank = __popc(rw[kp.word & (RBW - 1)] & ((1u << kp.bit) - 1u));
+            for (int k = 0; k < int(kp.word & (RBW - 1)); ++k) rank += __popc(rw[k]);
+            seg = uint32_t(kp.seg);
+        });
     }
 }
 
 // ---------------------------------------------------------------------------------------------
 // Label resolve and write.
 // ---------------------------------------------------------------------------------------------
+constexpr int kNLCap = 512;   // node links a write CTA stages in shared memory (later ones: from L2)
+
 __global__ void __launch_bounds__(NT, 5) k_tile_write_3d(ImgList3D L, Work w)
 {
     __shared__ __align__(16) uint32_t Ls[NBLK];
     __shared__ uint32_t LT[NBLK];
-    __shared__ uint32_t RB[TX * TY * RBW];
-    __shared__ uint32_t segb[TX * TY];
+    __shared__ __align__(16) uint32_t RB[TX * TY * RBW];
+    __shared__ uint32_t segb[TX * TY + 1];   // segment prefixes of the tile's voxel rows; [TX * TY]: the volume's first
+    __shared__ __align__(16) uint2 NL[kNLCap];
+    __shared__ uint32_t snb;
     __shared__ uint32_t qslot;
 
     const int tid = threadIdx.x;
     const uint32_t *lab = reinterpret_cast<const uint32_t *>(w.lab);
-    // Block entries and root bitmaps were final before this grid's predecessor (the scan and
-    // flatten) started: that grid waits for the merge to complete before it lets this one launch.
-    // So both are read before the wait (through L2); the segment prefixes and the flattened node
-    // links, which the predecessor writes, come after it.  With a fixed tile order (no work queue)
-    // the CTA loads its next tile's block entries and bitmap into registers while it writes the
-    // current tile's labels.
     static_assert(NBLK / 4 == 4 * NT && TX * TY * RBW == 4 * NT, "four prefetched words per thread");
+    static_assert(TX * TY == 2 * NT && kNLCap == 2 * NT, "two segment prefixes and two node links per thread");
+    // Block entries, root bitmaps and node counts were final before this grid's predecessor (the
+    // scan and link pass) started: that grid waits for the merge to complete before it lets this
+    // one launch.  So they are read before the wait -- the entries into registers, the bitmap and
+    // count into shared memory (cp.async) -- and the segment prefixes and node links, which the
+    // predecessor writes, are copied after it.  With a fixed tile order (no work queue) the next
+    // tile's fetches are issued before the current tile's labels are written.
     uint4 nL[4];
-    uint32_t nR[4];
     auto fetch = [&](int64_t t) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            nL[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + tid + i * NT);
-            nR[i] = __ldcg(w.rbits + t * (TX * TY * RBW) + tid + i * NT);
+        for (int i = 0; i < 4; ++i) nL[i] = __ldcg(reinterpret_cast<const uint4 *>(lab + t * NBLK) + tid + i * NT);
+        cp_async16(&RB[4 * tid], w.rbits + t * (TX * TY * RBW) + 4 * tid);
+        if (tid == NT - 1) cp_async4(&snb, w.nb + t);
+        cp_async_commit();
+    };
+    auto fetch_links = [&](int64_t t) {
+        const Img3D im = L.get(t);
+        const TileGeo g = tile_geo(im, t);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int r = tid + i * NT;
+            cp_async8(&NL[r], w.nlink + t * MAXB + r);
+            const int X = r / TY, Y = r % TY;
+            if (X < g.nx && Y < g.ny)
+                cp_async4(&segb[r], w.segpref + im.seg_base + (int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.t2 + g.tx2);
         }
+        if (tid == 0) cp_async4(&segb[TX * TY], w.segpref + im.seg_base);
+        cp_async_commit();
     };
     const bool fixed_order = w.queue == nullptr;
     ItemLoop loop{w.queue ? w.queue + 4 : nullptr, w.n_tiles};
@@ -956,26 +993,18 @@ __global__ void __launch_bounds__(NT, 5) k_tile_write_3d(ImgList3D L, Work w)
     if (t < w.n_tiles) fetch(t);
     for (bool first = true; t < w.n_tiles; t = loop.next(t, &qslot), first = false) {
         if (!fixed_order && !first) fetch(t);   // a work queue gives the next tile only now
+        if (first) grid_dep_wait();   // segment prefixes and node links from here on
+        if (first || !fixed_order) fetch_links(t);
         const Img3D im = L.get(t);
         const TileGeo g = tile_geo(im, t);
         const int64_t rs0 = int64_t(im.d1) * im.d2;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            reinterpret_cast<uint4 *>(Ls)[tid + i * NT] = nL[i];
-            RB[tid + i * NT] = nR[i];
-        }
-        if (fixed_order && t + gridDim.x < w.n_tiles) fetch(t + gridDim.x);
-        const uint32_t nb = __ldcg(w.nb + t);
-        grid_dep_wait();   // segment prefixes from here on (returns at once after the first tile)
-        const uint32_t base0 = w.segpref[im.seg_base];
-        for (int r = tid; r < TX * TY; r += NT) {
-            const int X = r / TY, Y = r % TY;
-            if (X < g.nx && Y < g.ny)
-                segb[r] = w.segpref[im.seg_base + (int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.t2 + g.tx2] - base0;
-        }
+        for (int i = 0; i < 4; ++i) reinterpret_cast<uint4 *>(Ls)[tid + i * NT] = nL[i];
+        cp_async_wait();
+        __syncthreads();
+        const uint32_t nb = snb, base0 = segb[TX * TY];
         if (t == im.tile_base && tid == 0)
             w.ncomp[im.index] = int64_t(w.segpref[im.seg_base + int64_t(im.d0) * im.d1 * im.t2] - base0);
-        __syncthreads();
         for (int b = tid; b < NBLK; b += NT) {
             const uint32_t e = Ls[b];
             if (!(e & ROOT_FLAG)) continue;
@@ -984,51 +1013,58 @@ __global__ void __launch_bounds__(NT, 5) k_tile_write_3d(ImgList3D L, Work w)
             const uint32_t *row = &RB[(X * TY + Y) * RBW];
             uint32_t rank = __popc(row[Z >> 5] & ((1u << (Z & 31)) - 1u));
             for (int k = 0; k < (Z >> 5); ++k) rank += __popc(row[k]);
-            LT[b] = 1u + segb[X * TY + Y] + rank;
+            LT[b] = 1u + (segb[X * TY + Y] - base0) + rank;
         }
         __syncthreads();
         // Border components linked under another tile's component: the label of that root, its
-        // segment's prefix plus its rank among the first voxels left in its row of its tile.
+        // segment's prefix plus its rank among the first voxels left there (both resolved by the
+        // link pass).
         for (uint32_t j = tid; j < nb; j += NT) {
-            const int64_t node = t * MAXB + j;
-            if (__ldcg(w.gp + node) == uint32_t(node)) continue;
-            const uint32_t gn = gfind_halve(w.gp, uint32_t(node));
-            const KeyPos kp = key_pos(im, __ldcg(w.nkey + gn));
-            if (!GUARD(w, kp.seg >= 0 && kp.seg < w.n_segs && kp.tile >= 0 && kp.tile < w.n_tiles, 404, kp.seg)) continue;
-            const uint32_t *rw = w.rbits + (kp.word & ~int64_t(RBW - 1));
-            uint32_t rank = __popc(__ldcg(rw + (kp.word & (RBW - 1))) & ((1u << kp.bit) - 1u));
-            for (int k = 0; k < int(kp.word & (RBW - 1)); ++k) rank += __popc(__ldcg(rw + k));
-            const uint32_t nr = __ldcg(w.nroot + node);
-            if (GUARD(w, nr < uint32_t(NBLK), 402, node)) LT[nr] = 1u + (w.segpref[kp.seg] - base0) + rank;
+            const uint2 e = j < uint32_t(kNLCap) ? NL[j] : __ldcg(w.nlink + t * MAXB + j);
+            if (e.x == kNone) continue;
+            const uint32_t nr = e.y >> 16;
+            if (GUARD(w, nr < uint32_t(NBLK) && e.x < w.n_segs, 402, t * MAXB + j))
+                LT[nr] = 1u + (__ldcg(w.segpref + e.x) - base0) + (e.y & 0xFFFFu);
         }
         __syncthreads();
+        if (fixed_order && t + gridDim.x < w.n_tiles) {   // RB, NL, segb and snb are free now
+            fetch(t + gridDim.x);
+            fetch_links(t + gridDim.x);
+        }
 
-        // Output: units of 4 voxels along d2 (2 blocks).
-        for (int u = tid; u < TX * TY * (TZ / 4); u += NT) {
-            const int q = u % (TZ / 4), r = u / (TZ / 4);
-            const int X = r / TY, Y = r % TY;
-            if (X >= g.nx || Y >= g.ny || 4 * q >= g.nz) continue;
-            const int bb = blk(X >> 1, Y >> 1, 2 * q);
-            const uint32_t e0 = Ls[bb], e1 = (2 * q + 1 < TB2) ? Ls[bb + 1] : 0u;
+        // Output: one unit = two blocks along d2 in all four voxel rows (X, Y) they cover: the two
+        // entries and labels are looked up once for four 16-byte stores.
+        for (int u = tid; u < TB0 * TB1 * (TB2 / 2); u += NT) {
+            const int q = u % (TB2 / 2), r = u / (TB2 / 2);
+            const int b0 = r / TB1, b1 = r % TB1;
+            if (2 * b0 >= g.nx || 2 * b1 >= g.ny || 4 * q >= g.nz) continue;
+            const int bb = blk(b0, b1, 2 * q);
+            const uint32_t e0 = Ls[bb], e1 = Ls[bb + 1];
             const uint32_t m0 = e0 >> 24, m1 = e1 >> 24;
             if (!GUARD(w, !m0 || (e0 & ROOT_FLAG) || (Ls[(e0 & 0x7FFFFFu) % NBLK] & ROOT_FLAG && (e0 & 0x7FFFFFu) < NBLK), 403, e0)) continue;
             const uint32_t l0 = m0 ? ((e0 & ROOT_FLAG) ? LT[bb] : LT[e0 & 0x7FFFFFu]) : 0u;
             const uint32_t l1 = m1 ? ((e1 & ROOT_FLAG) ? LT[bb + 1] : LT[e1 & 0x7FFFFFu]) : 0u;
-            const int sh = 4 * (X & 1) + 2 * (Y & 1);
-            int4 v;
-            v.x = ((m0 >> sh) & 1u) ? int(l0) : 0;
-            v.y = ((m0 >> (sh + 1)) & 1u) ? int(l0) : 0;
-            v.z = ((m1 >> sh) & 1u) ? int(l1) : 0;
-            v.w = ((m1 >> (sh + 1)) & 1u) ? int(l1) : 0;
-            int32_t *dst = im.out + (g.x0 + X) * rs0 + int64_t(g.y0 + Y) * im.d2 + g.z0 + 4 * q;
-            if (4 * q + 4 <= g.nz && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
-                __stcs(reinterpret_cast<int4 *>(dst), v);
-            } else {
-                const int n = min(4, g.nz - 4 * q);
-                dst[0] = v.x;
-                if (n > 1) dst[1] = v.y;
-                if (n > 2) dst[2] = v.z;
-                if (n > 3) dst[3] = v.w;
+            const bool full = 4 * q + 4 <= g.nz;
+#pragma unroll
+            for (int ij = 0; ij < 4; ++ij) {
+                const int X = 2 * b0 + (ij >> 1), Y = 2 * b1 + (ij & 1);
+                if (X >= g.nx || Y >= g.ny) continue;
+                const int sh = 2 * ij;   // mask bit of voxel (i, j, k) is 4i + 2j + k
+                int4 v;
+                v.x = ((m0 >> sh) & 1u) ? int(l0) : 0;
+                v.y = ((m0 >> (sh + 1)) & 1u) ? int(l0) : 0;
+                v.z = ((m1 >> sh) & 1u) ? int(l1) : 0;
+                v.w = ((m1 >> (sh + 1)) & 1u) ? int(l1) : 0;
+                int32_t *dst = im.out + (g.x0 + X) * rs0 + int64_t(g.y0 + Y) * im.d2 + g.z0 + 4 * q;
+                if (full && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+                    __stcs(reinterpret_cast<int4 *>(dst), v);
+                } else {
+                    const int n = min(4, g.nz - 4 * q);
+                    dst[0] = v.x;
+                    if (n > 1) dst[1] = v.y;
+                    if (n > 2) dst[2] = v.z;
+                    if (n > 3) dst[3] = v.w;
+                }
             }
         }
         __syncthreads();
