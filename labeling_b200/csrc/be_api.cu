@@ -70,8 +70,7 @@ size_t layout_work(const Geometry &g, int64_t n_tiles, int64_t n_segs, int n_img
     t.perim = reinterpret_cast<uint16_t *>(take(size_t(n_tiles) * g.nperim * sizeof(uint16_t)));
     t.rbits = reinterpret_cast<uint32_t *>(take(size_t(n_tiles) * g.rbits_bytes_per_tile));
     t.nb = reinterpret_cast<uint32_t *>(take(size_t(n_tiles) * sizeof(uint32_t)));
-    t.gp = reinterpret_cast<uint32_t *>(take(nodes * sizeof(uint32_t)));
-    t.nkey = reinterpret_cast<uint32_t *>(take(nodes * sizeof(uint32_t)));
+    t.gp = reinterpret_cast<unsigned long long *>(take(nodes * sizeof(unsigned long long)));
     t.nroot = reinterpret_cast<uint16_t *>(take(nodes * sizeof(uint16_t)));
     t.nlink = g.links ? reinterpret_cast<uint2 *>(take(nodes * sizeof(uint2))) : nullptr;
     t.segcnt = reinterpret_cast<uint8_t *>(take(align_up(size_t(n_segs), 16) + 16));

@@ -63,8 +63,8 @@ struct Work {
     void *lab;            // per-block tile-local labels: uint16 (2D) / uint32 (3D), NBLK per tile
     uint16_t *perim;      // per tile NPERIM border entries: (node << 4) | side bits, 0 = empty
     uint32_t *nb;         // per tile: number of nodes
-    uint32_t *gp;         // per node (tile * MAXB + j): union-find parent (global node id)
-    uint32_t *nkey;       // per node: key of the node's root pixel
+    unsigned long long *gp;   // per node (tile * MAXB + j): union-find entry (key of the parent << 32) |
+                              // parent (global node id); see gentry
     uint16_t *nroot;      // per node: tile-local block index of the node's root block
     uint2 *nlink;         // per node, after the merge: x = segment of its global root's first pixel
                           // (kNone when the node is a root itself), y = (root block << 16) | rank
@@ -219,81 +219,89 @@ __device__ __forceinline__ uint32_t warp_reserve(uint32_t *count, uint32_t n)
     return base + incl - n;
 }
 
-// Union of two nodes by key: the root with the larger key is linked under the other, so parent
-// keys strictly decrease along every path and no link can close a cycle, whatever other threads
-// link meanwhile.  Latency, not work, is the cost (each step is an L2 round trip), so both finds
-// walk in lockstep (one round trip per step for both paths), and the first round trip also
-// fetches both keys, which are final when the two nodes are still roots.  on_link(key) is called
-// with the key of the root that was linked.
-template <typename OnLink>
-__device__ __forceinline__ void gunion_keyed(uint32_t *gp, const uint32_t *nkey, uint32_t a, uint32_t b,
-                                             OnLink on_link)
+// Global union-find entries: gp[x] = (key of x's parent << 32) | parent, a root holding its own key
+// and index.  Keys (first-pixel raster indices) are distinct, and a parent's key is always smaller
+// than its child's, so no path can close a cycle whatever other threads link meanwhile, and one
+// load of an entry gives both the parent and the key that decides which way a union goes.
+__device__ __forceinline__ unsigned long long gentry(uint32_t key, uint32_t id)
 {
-    volatile uint32_t *vp = gp;
-    uint32_t pa = vp[a], pb = vp[b];
-    uint32_t ka = __ldg(nkey + a), kb = __ldg(nkey + b);
+    return (static_cast<unsigned long long>(key) << 32) | id;
+}
+
+// Union of nodes a and b after Rem's algorithm, lock-free: the two sides climb in turn, always
+// the side whose parent has the larger key (the order keys are linked in), with path halving on
+// the way; the walk ends where the two parents meet (already one set), or when the climbing side
+// stands on a root, which is linked (CAS) under the other side's parent -- a node of b's set with
+// a smaller key.  A walk that reaches the common ancestor stops there instead of going on to both
+// roots.  Latency, not work, is the cost: each step is one L2 round trip, and one load gives the
+// parent and its key.  on_link(key) is called with the key of the root that was linked.  (Rem's
+// splicing -- re-pointing the climbing node at the other side's parent -- was measured: it merged
+// the long paths of one-pixel spirals into deep trees.)
+template <typename OnLink>
+__device__ __forceinline__ void gunion_keyed(unsigned long long *gp, uint32_t a, uint32_t b, OnLink on_link)
+{
+    volatile unsigned long long *vp = gp;
+    unsigned long long ea = vp[a], eb = vp[b];
     for (;;) {
-        bool moved_a = false, moved_b = false;
-        while (pa != a || pb != b) {
-            const uint32_t ga = pa != a ? vp[pa] : pa;
-            const uint32_t gb = pb != b ? vp[pb] : pb;
-            if (pa != a) {
-                if (ga != pa) vp[a] = ga;   // path halving: only ever an ancestor
-                a = pa;
-                pa = ga;
-                moved_a = true;
+        if (uint32_t(ea) == uint32_t(eb)) return;   // same parent: one set
+        if ((ea >> 32) < (eb >> 32)) {               // climb on the side with the larger parent key
+            const uint32_t t = a; a = b; b = t;
+            const unsigned long long u = ea; ea = eb; eb = u;
+        }
+        const uint32_t pa = uint32_t(ea);
+        if (pa == a) {   // a root
+            const unsigned long long old = atomicCAS(gp + a, ea, eb);
+            if (old == ea) {
+                on_link(uint32_t(ea >> 32));
+                return;
             }
-            if (pb != b) {
-                if (gb != pb) vp[b] = gb;
-                b = pb;
-                pb = gb;
-                moved_b = true;
-            }
+            ea = old;
+            eb = vp[b];
+            continue;
         }
-        if (a == b) return;
-        if (moved_a) ka = __ldg(nkey + a);
-        if (moved_b) kb = __ldg(nkey + b);
-        if (ka < kb) {
-            uint32_t t = a; a = b; b = t;
-            t = ka; ka = kb; kb = t;
-        }
-        const uint32_t old = atomicCAS(gp + a, a, b);
-        if (old == a) {
-            on_link(ka);
-            return;
-        }
-        // a was linked meanwhile: go on from its new parent, and re-read b too (linking under a
-        // stale b would stay correct but deepen the trees that every later find walks).
-        pa = old;
-        pb = vp[b];
+        const unsigned long long ga = vp[pa];
+        if (uint32_t(ga) != pa) vp[a] = ga;   // halving
+        a = pa;
+        ea = ga;
     }
 }
 
 // Find with path halving after all merges of the launch are complete: no link can happen any more,
 // so every pointer stored is to an ancestor and any interleaving of the stores keeps the trees
 // valid.  The cap only bounds the walk should the forest ever hold a cycle (it cannot).
-__device__ __forceinline__ uint32_t gfind_halve(uint32_t *gp, uint32_t a)
+__device__ __forceinline__ uint32_t gfind_halve(unsigned long long *gp, uint32_t a)
 {
-    volatile uint32_t *vp = gp;
-    uint32_t p = vp[a];
-    for (int it = 0; p != a && it < (1 << 24); ++it) {
-        const uint32_t g = vp[p];
-        if (g != p) vp[a] = g;
+    volatile unsigned long long *vp = gp;
+    unsigned long long e = vp[a];
+    for (int it = 0; uint32_t(e) != a && it < (1 << 24); ++it) {
+        const uint32_t p = uint32_t(e);
+        const unsigned long long g = vp[p];
+        if (uint32_t(g) != p) vp[a] = g;
         a = p;
-        p = g;
+        e = g;
     }
     return a;
 }
 
-// Read-only find (after all merges of the launch are complete).
-__device__ __forceinline__ uint32_t gfind_ro(const uint32_t *gp, uint32_t a)
+// Root of node x after all merges of the launch are complete, by pointer jumping that writes only
+// x's own entry: each step x is pointed at its parent's parent as that entry reads now.  When every
+// node of a deep tree runs this at once, each read lands on an entry that its own thread has
+// already shortened, so the walks take about log2(depth) steps instead of depth (and no two
+// threads write the same entry).  The cap only bounds the walk should the forest ever hold a cycle
+// (it cannot).
+__device__ __forceinline__ uint32_t gfind_jump(unsigned long long *gp, uint32_t x)
 {
-    uint32_t p = gp[a];
-    while (p != a) {
-        a = p;
-        p = gp[a];
+    volatile unsigned long long *vp = gp;
+    uint32_t p = uint32_t(vp[x]);
+    if (p == x) return x;
+    for (int it = 0; it < (1 << 24); ++it) {
+        const unsigned long long ep = vp[p];
+        const uint32_t g = uint32_t(ep);
+        if (g == p) break;   // p is the root
+        vp[x] = ep;
+        p = g;
     }
-    return a;
+    return p;
 }
 
 // ---- Border-merge filter ---------------------------------------------------------------------

@@ -35,7 +35,7 @@ constexpr size_t kScratchBytes =
     al256(kMaxTiles * T2_NPERIM * 2) +                            // border entries
     al256(kMaxTiles * (2 * T2_TBH) * (2 * T2_TBW / 32) * 4) +     // root bitmaps
     al256(kMaxTiles * 4) +                                        // node counts
-    2 * al256(kMaxTiles * T2_MAXB * 4) +                          // parent, key
+    al256(kMaxTiles * T2_MAXB * 8) +                              // union-find entries
     al256(kMaxTiles * T2_MAXB * 2) +                              // root block
     al256((kMaxSegs + 15) / 16 * 16 + 16) +                       // segment counts
     al256((kMaxSegs + 1) * 4) +                                   // segment prefix

@@ -129,20 +129,17 @@ __device__ __forceinline__ void segscan_lb_chunk(Work &w, uint32_t *tmp, uint32_
     if (c == w.n_chunks - 1 && threadIdx.x == 0) w.segpref[w.n_segs] = sh_excl + ctot;
 }
 
-// Points every linked node of tile t straight at its global root: all unions are done, so every
-// writer stores the same final root and any interleaving is safe.  Called by a whole CTA.
+// Points every linked node of tile t at its global root (gfind_jump: the nodes of all tiles jump
+// at once, each writing only its own entry, so deep trees take logarithmic walks).  Called by a
+// whole CTA.
 __device__ __forceinline__ void flatten_tile_nodes(Work &w, int64_t t, int maxb)
 {
     const uint32_t nb = w.nb[t];
     for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
         const uint32_t node = uint32_t(t * maxb + j);
-        if (w.gp[node] == node) continue;
-        const uint32_t root = gfind_ro(w.gp, node);
-        for (uint32_t y = node; y != root;) {
-            const uint32_t ny = w.gp[y];
-            w.gp[y] = root;
-            y = ny;
-        }
+        if (uint32_t(w.gp[node]) == node) continue;
+        const uint32_t root = gfind_jump(w.gp, node);
+        w.gp[node] = w.gp[root];
     }
 }
 
@@ -158,15 +155,12 @@ __device__ __forceinline__ void link_tile_nodes(Work &w, int64_t t, int maxb, Lo
     for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
         const uint32_t node = uint32_t(t * maxb + j);
         uint2 link = make_uint2(kNone, 0u);
-        if (w.gp[node] != node) {
-            const uint32_t root = gfind_ro(w.gp, node);
-            for (uint32_t y = node; y != root;) {
-                const uint32_t ny = w.gp[y];
-                w.gp[y] = root;
-                y = ny;
-            }
+        if (uint32_t(w.gp[node]) != node) {
+            const uint32_t root = gfind_jump(w.gp, node);
+            const unsigned long long re = w.gp[root];
+            w.gp[node] = re;
             uint32_t seg, rank;
-            locate(w.nkey[root], seg, rank);
+            locate(uint32_t(re >> 32), seg, rank);
             link = make_uint2(seg, (uint32_t(w.nroot[node]) << 16) | rank);
         }
         w.nlink[node] = link;

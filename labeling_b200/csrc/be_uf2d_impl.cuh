@@ -523,9 +523,9 @@ __global__ void __launch_bounds__(K1_NT, 8) k_tile_local_2d(ImgList2D L, Work w)
                 first_px(M[rb], dy, dx);
                 const int y = 2 * int(rb / TBW) + dy, x = 2 * int(rb % TBW) + dx;
                 const int64_t node = t * MAXB + j;
+                const uint32_t key = uint32_t(int64_t(y0 + y) * im.cols + (x0 + x));
                 w.nroot[node] = uint16_t(rb);
-                w.nkey[node] = uint32_t(int64_t(y0 + y) * im.cols + (x0 + x));
-                w.gp[node] = uint32_t(node);
+                w.gp[node] = gentry(key, uint32_t(node));
             }
             w.perim[t * NPERIM + p] = ent;
         }
@@ -555,13 +555,14 @@ __device__ __forceinline__ void link_dec(const Img2D &im, Work &w, uint32_t key)
 // the linked root leaves its segment's root count and its tile's root bitmap.
 __device__ void gunion2d(const Img2D &im, Work &w, uint32_t a, uint32_t b)
 {
-    gunion_keyed(w.gp, w.nkey, a, b, [&](uint32_t key) { link_dec(im, w, key); });
+    gunion_keyed(w.gp, a, b, [&](uint32_t key) { link_dec(im, w, key); });
 }
 
 }  // namespace
 
 constexpr int K2_NP = TBH + TBW;               // border positions a merge CTA looks at
 constexpr int K2_NT = 64;                      // threads of a merge CTA (small: many tiles per SM)
+constexpr int K2_PER_SM = 28;                  // resident merge CTAs per SM
 constexpr int kGQ2 = 256;                      // queued global unions per tile (more are done at once)
 constexpr int SR = MAXB;                       // local index of the staged right column
 constexpr int SD = MAXB + TBH;                 // local index of the staged bottom row (column -1 first)
@@ -576,7 +577,7 @@ constexpr int NLOC2 = MAXB + TBH + TBW + 2;    // local union-find size
 // union-find, from a shared queue once all of the tile's pairs are seen.  The merge is bound by
 // the latency of those global unions (dependent L2 round trips), so a CTA is two warps that loop
 // over the positions: many tiles are in flight on each SM at once.
-__global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
+__global__ void __launch_bounds__(K2_NT, K2_PER_SM) k_merge_2d(ImgList2D L, Work w)
 {
     grid_dep_wait();
     grid_dep_release();
@@ -585,6 +586,7 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
     __shared__ uint32_t sid[TBH + TBW + 2];   // staged global node ids (kNone = none)
     __shared__ uint8_t smk[TBH + TBW + 2];    // staged masks
     __shared__ uint16_t own[K2_NP];           // this tile's own border entries
+    __shared__ uint8_t cm[K2_NP];             // connected staged neighbours of each position
     __shared__ uint2 gq[kGQ2];
     __shared__ uint32_t nq;
     ItemLoop loop{w.queue ? w.queue + 1 : nullptr, w.n_tiles};
@@ -640,19 +642,60 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
             own[p] = A;
         }
         __syncthreads();
-        // Neighbouring staged positions of one node are one element.
-        for (int p = threadIdx.x; p < K2_NP; p += K2_NT) {
-            if (p < TBH) {
-                if (p > 0 && sid[p] != kNone && sid[p] == sid[p - 1]) smerge(lp, uint32_t(SR + p), uint32_t(SR + p - 1));
-            } else {
-                const int k = p - TBH + 1;   // staged bottom index, column k - 1
-                if (sid[TBH + k] != kNone && sid[TBH + k] == sid[TBH + k - 1])
-                    smerge(lp, uint32_t(SD + k), uint32_t(SD + k - 1));
-                if (p == TBH && sid[TBH + TBW + 1] != kNone && sid[TBH + TBW + 1] == sid[TBH + TBW])
-                    smerge(lp, uint32_t(SD + TBW + 1), uint32_t(SD + TBW));
+        // Neighbouring staged positions of one node are one element: every position of a run of
+        // equal node ids along the staged column (warp 0) or row (warp 1) points at the run's first
+        // position, found by ballots 32 positions at a time (no merging, no chains).
+        {
+            const int lane = threadIdx.x & 31;
+            const int lo = threadIdx.x < 32 ? 0 : TBH, n = threadIdx.x < 32 ? TBH : TBW + 2;
+            uint32_t carry = 0;
+            for (int c0 = 0; c0 < n; c0 += 32) {
+                const int k = c0 + lane;
+                const bool valid = k < n;
+                const bool start = valid && (k == 0 || sid[lo + k] != sid[lo + k - 1]);
+                const uint32_t below = __ballot_sync(0xFFFFFFFFu, start) & (0xFFFFFFFFu >> (31 - lane));
+                const uint32_t st = below ? uint32_t(c0) + hibit(below) : carry;
+                if (valid) lp[MAXB + lo + k] = uint32_t(MAXB + lo) + st;
+                carry = __shfl_sync(0xFFFFFFFFu, st, 31);
             }
         }
+        // Connected neighbours of every position: bit d + 1 for the staged neighbour at offset d.
+        for (int p = threadIdx.x; p < K2_NP; p += K2_NT) {
+            const uint32_t A = own[p];
+            uint32_t cb = 0;
+            if (A) {
+                const uint32_t mA = A & 15u;
+                if (p < TBH) {
+                    // Right border: neighbours in the tile to the right, same tile row.
+#pragma unroll
+                    for (int d = -1; d <= 1; ++d) {
+                        const int rr = p + d;
+                        if (rr < 0 || rr >= nbr || sid[rr] == kNone) continue;
+                        const uint32_t mB = smk[rr];
+                        if (d == 0 ? ((mA & 0xAu) && (mB & 0x5u)) : d < 0 ? ((mA & 2u) && (mB & 4u)) : ((mA & 8u) && (mB & 1u)))
+                            cb |= 1u << (d + 1);
+                    }
+                } else {
+                    // Bottom border: neighbours in the tile row below (including the diagonal tiles).
+                    const int c = p - TBH;
+#pragma unroll
+                    for (int d = -1; d <= 1; ++d) {
+                        const int k = c + d + 1;   // staged bottom index
+                        if (sid[TBH + k] == kNone) continue;
+                        const uint32_t mB = smk[TBH + k];
+                        if (d == 0 ? ((mA & 0xCu) && (mB & 0x3u)) : d < 0 ? ((mA & 4u) && (mB & 2u)) : ((mA & 8u) && (mB & 1u)))
+                            cb |= 1u << (d + 1);
+                    }
+                }
+            }
+            cm[p] = uint8_t(cb);
+        }
         __syncthreads();
+        // Pairs.  Staged index of a position's neighbour at offset d: p + d on the right border,
+        // TBH + c + d + 1 on the bottom border.  A pair is skipped when the position before (same
+        // border, same own node) touches the same staged run: that position's pair stands for it.
+        // A pair that passes goes through the CTA-local union-find, and only one that joins two
+        // local sets goes on to the global union-find.
         auto pair = [&](uint32_t ja, uint32_t nA, uint32_t le, uint32_t nB) {
             if (!smerge_joined(lp, ja, le)) return;
             const uint32_t slot = atomicAdd(&nq, 1u);
@@ -661,42 +704,27 @@ __global__ void __launch_bounds__(K2_NT) k_merge_2d(ImgList2D L, Work w)
         };
         for (int p = threadIdx.x; p < K2_NP; p += K2_NT) {
             const uint32_t A = own[p];
-            if (!A) continue;
-            const uint32_t mA = A & 15u, ja = A >> 4, nA = uint32_t(t * MAXB + ja);
+            uint32_t cb = cm[p];
+            if (!A || !cb) continue;
+            const uint32_t ja = A >> 4, nA = uint32_t(t * MAXB + ja);
+            const int i0 = p < TBH ? p : p + 1;   // staged index of the neighbour at offset d: i0 + d
+            // the position before on the same border, when it belongs to the same own node
+            const bool prev = p != 0 && p != TBH && own[p - 1] && (own[p - 1] >> 4) == ja;
+            const uint32_t cbp = prev ? cm[p - 1] : 0u;
             uint32_t lastB = kNone;   // a node already paired with this one needs no second pair
-            if (p < TBH) {
-                // Right border: neighbours in the tile to the right, same tile row.
-                const int r = p;
+            while (cb) {
+                const int d = __ffs(cb) - 2;
+                cb &= cb - 1;
+                const int i = i0 + d;
+                const uint32_t nB = sid[i], rs = lp[MAXB + i];
+                if (nB == lastB) continue;
+                bool seen = false;
 #pragma unroll
-                for (int d = -1; d <= 1; ++d) {
-                    const int rr = r + d;
-                    if (rr < 0 || rr >= nbr) continue;
-                    const uint32_t nB = sid[rr];
-                    if (nB == kNone || nB == lastB) continue;
-                    const uint32_t mB = smk[rr];
-                    const bool c = d == 0 ? ((mA & 0xAu) && (mB & 0x5u))
-                                          : d < 0 ? ((mA & 2u) && (mB & 4u)) : ((mA & 8u) && (mB & 1u));
-                    if (c) {
-                        pair(ja, nA, uint32_t(SR + rr), nB);
-                        lastB = nB;
-                    }
-                }
-            } else {
-                // Bottom border: neighbours in the tile row below (including the diagonal tiles).
-                const int c = p - TBH;
-#pragma unroll
-                for (int d = -1; d <= 1; ++d) {
-                    const int k = c + d + 1;   // staged bottom index
-                    const uint32_t nB = sid[TBH + k];
-                    if (nB == kNone || nB == lastB) continue;
-                    const uint32_t mB = smk[TBH + k];
-                    const bool cn = d == 0 ? ((mA & 0xCu) && (mB & 0x3u))
-                                           : d < 0 ? ((mA & 4u) && (mB & 2u)) : ((mA & 8u) && (mB & 1u));
-                    if (cn) {
-                        pair(ja, nA, uint32_t(SD + k), nB);
-                        lastB = nB;
-                    }
-                }
+                for (int dp = -1; dp <= 1; ++dp)
+                    if ((cbp >> (dp + 1)) & 1u) seen |= lp[MAXB + i0 - 1 + dp] == rs;
+                if (seen) continue;
+                pair(ja, nA, rs, nB);
+                lastB = nB;
             }
         }
         __syncthreads();
@@ -815,9 +843,9 @@ __global__ void __launch_bounds__(K3_NT, 8) k_tile_write_2d(ImgList2D L, Work w)
         // segment's prefix plus its rank among the first pixels left in its row of its tile.
         for (uint32_t j = tid; j < nb; j += K3_NT) {
             const int64_t node = t * MAXB + j;
-            if (__ldcg(w.gp + node) == uint32_t(node)) continue;
+            if (uint32_t(__ldcg(w.gp + node)) == uint32_t(node)) continue;
             const uint32_t g = gfind_halve(w.gp, uint32_t(node));
-            const uint32_t kg = __ldcg(w.nkey + g);
+            const uint32_t kg = uint32_t(__ldcg(w.gp + g) >> 32);
             const int64_t yg = kg / uint32_t(im.cols), xg = kg - yg * im.cols;
             const int64_t tyg = yg / TH, txg = xg / TW;
             const int ly = int(yg - tyg * TH), lx = int(xg - txg * TW);
@@ -898,7 +926,7 @@ inline cudaError_t launch(const ImgList2D &L, const Work &w, int sms, bool persi
     k_tile_local_2d<<<grid(w.n_tiles, 8), K1_NT, 0, s>>>(L, wk);
     keep(cudaGetLastError());
     mark(1);
-    keep(launch_k(k_merge_2d, grid(w.n_tiles, 28), K2_NT, s, ov, L, wk));
+    keep(launch_k(k_merge_2d, grid(w.n_tiles, K2_PER_SM), K2_NT, s, ov, L, wk));
     mark(2);
     keep(launch_k(k_scan_flatten_2d, grid(int64_t(w.n_chunks) + w.n_tiles, 8), kScanThreads, s, ov, wk));
     mark(3);

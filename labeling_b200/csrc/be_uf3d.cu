@@ -598,9 +598,9 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
                     break;
                 const int Z = key % TZ, Y = (key / TZ) % TY, X = key / (TZ * TY);
                 const int64_t node = t * MAXB + j;
+                const uint32_t vkey = uint32_t((int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.d2 + (g.z0 + Z));
                 w.nroot[node] = uint16_t(rb);
-                w.nkey[node] = uint32_t((int64_t(g.x0 + X) * im.d1 + (g.y0 + Y)) * im.d2 + (g.z0 + Z));
-                w.gp[node] = uint32_t(node);
+                w.gp[node] = gentry(vkey, uint32_t(node));
                 ++j;
             }
         }
@@ -650,7 +650,7 @@ __device__ __forceinline__ KeyPos key_pos(const Img3D &im, uint32_t key)
 // count and its tile's root bitmap.
 __device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
 {
-    gunion_keyed(w.gp, w.nkey, a, b, [&](uint32_t key) {
+    gunion_keyed(w.gp, a, b, [&](uint32_t key) {
         const KeyPos kp = key_pos(im, key);
         dec_u8(w.segcnt, kp.seg);
         atomicAnd(w.rbits + kp.word, ~(1u << kp.bit));
