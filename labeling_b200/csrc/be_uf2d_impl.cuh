@@ -416,10 +416,11 @@ __global__ void __launch_bounds__(K1_NT, 8) k_tile_local_2d(ImgList2D L, Work w)
             }
         }
 
-        // Phase C: every run start of this word, and every entry on its path, points straight at
-        // its root (a read-only walk, then the root's entry stored along the path: every writer
-        // stores the same final entry, and no link happens any more); roots mark their first
-        // pixel.  Then the block entries: (mask << 12) | root block, two blocks per 32-bit word.
+        // Phase C: every run start of this word is pointed straight at its root (a read-only walk,
+        // then the root's entry stored in the start's own entry; every entry is a run start, so each
+        // is compressed by its own thread, and no link happens any more -- storing the root along
+        // the walked path as well was measured slower: a second dependent walk); roots mark their
+        // first pixel.  Then the block entries: (mask << 12) | root block, two blocks per 32-bit word.
         {
             uint32_t ss = S;
             while (ss) {
@@ -430,11 +431,7 @@ __global__ void __launch_bounds__(K1_NT, 8) k_tile_local_2d(ImgList2D L, Work w)
                     root = ev & 0xFFFu;
                     ev = P[sw(root)];
                 }
-                for (uint32_t y = x, it = 0; y != root && it < NBLK; ++it) {
-                    const uint32_t ny = P[sw(y)] & 0xFFFu;
-                    P[sw(y)] = ev;
-                    y = ny;
-                }
+                if (root != x) P[sw(x)] = ev;
                 if (root == x) {
                     const uint32_t key = ev >> 12;
                     const uint32_t rb = key_block(key);

@@ -490,9 +490,9 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
             }
         }
 
-        // Phase C: every run start of this row, and every entry on its path, points straight at its
-        // root (a read-only walk, then the root's entry stored along the path: every writer stores
-        // the same final entry); roots mark their first voxel.
+        // Phase C: every run start of this row is pointed straight at its root (a read-only walk,
+        // then the root's entry stored in the start's own entry, as in 2D); roots mark their first
+        // voxel.
         {
             uint32_t ss = S;
             while (ss) {
@@ -503,11 +503,7 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
                     root = ev & 0xFFFu;
                     ev = P[sw3(root)];
                 }
-                for (uint32_t y = x, it = 0; y != root && it < NBLK; ++it) {
-                    const uint32_t ny = P[sw3(y)] & 0xFFFu;
-                    P[sw3(y)] = ev;
-                    y = ny;
-                }
+                if (root != x) P[sw3(x)] = ev;
                 if (root != x) continue;
                 const uint32_t rb = slot_block(ev >> 12);
                 const uint32_t key = local_key(int(rb), M[rb]);
