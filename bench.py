@@ -44,7 +44,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 STAGES_2D = ["k_tile_local_2d", "k_merge_2d", "k_scan_flatten_2d", "k_tile_write_2d"]
-STAGES_3D = ["k_tile_local_3d", "k_merge_3d", "k_scan_flatten_3d", "k_tile_write_3d"]
+STAGES_3D = ["k_tile_local_3d", "k_merge_3d", "k_scan_link_3d", "k_tile_write_3d"]
 # Algorithmic bytes per pixel of each launch (what the launch must move at minimum):
 # tile_local reads the image (1 B), tile_write writes the labels (4 B); the others move only
 # per-tile / per-segment metadata and have no per-pixel algorithmic traffic.
@@ -62,6 +62,7 @@ IMPL_BYTES = {
            "segment counts + prefix": (1 + 1 + 4 + 4) / 256},
     "3d": {"input read": 1.0, "labels written": 4.0,
            "block entries written + read (uint32 per 2x2x2 block)": 2 * 0.5,
+           "root bitmap written + read (1 bit per voxel)": 2 * 0.125,
            "border entries written + read twice": 3 * 2 * (8 * 16 + 8 * 32 + 16 * 32) * 2 / 32768,
            "segment counts + prefix": (1 + 1 + 4 + 4) / 64},
 }
