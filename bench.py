@@ -1,11 +1,14 @@
 """Benchmark of the B200 Block-Equivalence labeler; prints ONE JSON line (rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload 2d8192|2d2048|3d512|batch|serve|slab2d] [--subs LIST] [--algo uf|iter]
+                    [--workload 2d8192|2d2048|3d512|batch|serve|slab2d] [--subs LIST]
+                    [--algo uf|iter|runs]
 
 Default run: the 2D 8192x8192 headline plus one sub-record per other configuration of the metric
 ("sub": 3D 512^3, the 4096-image uneven batch against 4096 plain launches, and the served Poisson
-sweep with p50 / p99), each with its own roofline, end-to-end figure and clock record.
+sweep with p50 / p99), each with its own roofline, end-to-end figure and clock record, and two
+more on the headline's images: the paper's iterative scan / analyze form ("iter") and the run
+equivalence form ("runs", 4-connected).
 
 Headline (2d8192): the seven seeded 8192x8192 families (Bernoulli p = 0.1 / 0.4 / 0.6 / 0.9, 2000
 disks over p = 0.05 noise, serpentine, spiral), 8-connectivity, int32 labels.  One step labels one
@@ -540,7 +543,9 @@ def bench_plain(args, rank, world, local_rank, workload):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         budget = 20.0
-        if is3d:
+        if not getattr(args, "cpu_leg", True):
+            pass   # a sub-record of the headline run: its CPU baseline is the headline's
+        elif is3d:
             result["cpu_baseline"] = cpu_reference_3d(inputs, budget)
         else:
             result["cpu_baseline"] = cpu_reference_2d(inputs, budget, "runeq" if algo == be.ALGO_RUNS else "bleq")
@@ -877,7 +882,7 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="2d8192", choices=["2d8192", "2d2048", "3d512", "batch", "serve", "slab2d"])
-    ap.add_argument("--subs", default="3d512,batch,serve",
+    ap.add_argument("--subs", default="3d512,batch,serve,iter,runs",
                     help="with the 2d8192 headline: the other configurations measured in the same run, "
                          "as sub-records (empty string: none)")
     ap.add_argument("--algo", default="uf", choices=["uf", "iter", "runs"],
@@ -926,6 +931,11 @@ def main():
                     r = bench_batch(args, rank, world, local_rank)
                 elif s == "serve":
                     r = bench_serve(args, rank, world, local_rank)
+                elif s in ("iter", "runs"):
+                    # the paper's iterative form / run equivalence on the headline's images
+                    a2 = argparse.Namespace(**vars(args))
+                    a2.algo, a2.cpu_leg = s, False
+                    r = bench_plain(a2, rank, world, local_rank, "2d8192")
                 else:
                     raise SystemExit(f"unknown sub-record {s}")
                 for k in ("higher_is_better", "scaling", "vs_baseline", "dtype", "data", "n_gpus"):
