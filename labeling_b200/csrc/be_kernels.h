@@ -26,7 +26,6 @@ __global__ void k_scan_link_3d(ImgList3D L, Work w);
 __global__ void k_tile_write_3d(ImgList3D L, Work w);
 
 __global__ void k_segscan(Work w);
-__global__ void k_segscan_lb(Work w);
 __global__ void k_chunk_sums(Work w);
 
 constexpr int kPostThreads = 128;   // k_chunk_sums

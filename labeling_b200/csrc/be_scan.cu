@@ -1,6 +1,6 @@
-// be_scan.cu -- exclusive scan of the per-segment root counts: k_segscan is the second half of
-// the two-launch scan of the iterative forms (the chunk sums run in k_chunk_sums), k_segscan_lb
-// the single-pass form the union-find pipelines fuse with their node flatten.
+// be_scan.cu -- exclusive scan of the per-segment root counts for the iterative forms: k_chunk_sums
+// sums each chunk, k_segscan scans them (the union-find pipelines use the single-pass scan of
+// be_scan.cuh inside their scan + node launch).
 #include "be_kernels.h"
 #include "be_scan.cuh"
 
@@ -63,18 +63,7 @@ __global__ void __launch_bounds__(kScanThreads) k_segscan(Work w)
     if (c == gridDim.x - 1 && threadIdx.x == 0) w.segpref[w.n_segs] = off + ctot;
 }
 
-// Single-pass scan of the segment counts (one CTA per chunk; see segscan_lb_chunk).
-__global__ void __launch_bounds__(kScanThreads) k_segscan_lb(Work w)
-{
-    // Release after the wait, as k_segscan: the label-write launch relies on it.
-    grid_dep_wait();
-    grid_dep_release();
-    __shared__ uint32_t tmp[kScanThreads / 32 + 1];
-    __shared__ uint32_t sh[2];
-    segscan_lb_chunk<kScanThreads>(w, tmp, sh);
-}
-
-// Chunk sums alone (one CTA per chunk), for pipelines without border roots to rank.
+// Chunk sums (one CTA per chunk), the first half of the two-launch scan.
 __global__ void __launch_bounds__(kPostThreads) k_chunk_sums(Work w)
 {
     __shared__ uint32_t tmp[kPostThreads / 32 + 1];
