@@ -178,31 +178,8 @@ __device__ __forceinline__ uint32_t slot_block(uint32_t slot)
 // -- reach 32 different banks.  Entries still name blocks by their plain index.
 __device__ __forceinline__ uint32_t sw3(uint32_t x) { return x ^ ((x >> 5) & 31u); }
 
-// Union-find over run starts, the slot carried in the entry: (slot << 12) | parent.
-__device__ __forceinline__ uint32_t efind3(uint32_t *P, uint32_t x)
-{
-    uint32_t v = P[sw3(x)];
-    while ((v & 0xFFFu) != x) {
-        const uint32_t y = v & 0xFFFu;
-        const uint32_t vg = P[sw3(y)];
-        if ((vg & 0xFFFu) != y) P[sw3(x)] = vg;
-        x = y;
-        v = vg;
-    }
-    return x;
-}
-
-__device__ __forceinline__ uint32_t efind3_ro(const uint32_t *P, uint32_t x)
-{
-    uint32_t v = P[sw3(x)];
-    while ((v & 0xFFFu) != x) {
-        x = v & 0xFFFu;
-        v = P[sw3(x)];
-    }
-    return x;
-}
-
-// As efind3, also returning the root's own entry as read (the union compares the two).
+// Union-find over run starts, the slot carried in the entry: (slot << 12) | parent.  The find
+// (path halving) returns the root and the root's own entry as read (the union compares the two).
 __device__ __forceinline__ uint32_t efind3_e(uint32_t *P, uint32_t x, uint32_t &ev)
 {
     uint32_t v = P[sw3(x)];
@@ -836,7 +813,8 @@ __global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Wo
             if (slot < uint32_t(kGQ3)) gq[slot] = make_uint2(nA, id);
             else gunion3d(im, w, nA, id);
         };
-        const uint32_t nbt = w.nb[t];
+        const uint32_t nbt = w.nb[t];   // (read by the bounds checks of checked builds)
+        (void)nbt;
         for (int base = 0; base < NPLUS; base += kT3MergeThreads) {
             const int p = base + int(threadIdx.x);
             int u = 0, v = 0, ebase = 0, pitch = 1;
