@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(K1_NT, 8) k_tile_local_2d(ImgList2D L, Work w)
             const uint32_t st = m ? (blk & ~31u) + hibit(m) : (blk & ~uint32_t(TBW - 1)) + WCS[blk >> 5];
             // A start of this tile by construction; the mask only keeps a broken invariant
             // from leaving the array.
-            GUARD(w, st < uint32_t(NBLK), 112, (uint64_t(blk) << 32) | st);
+            (void)GUARD(w, st < uint32_t(NBLK), 112, (uint64_t(blk) << 32) | st);
             return st & (NBLK - 1);
         };
         const uint32_t ubase = rbase - TBW + 32 * q, abase = rbase + 32 * q;
@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(K1_NT, 8) k_tile_local_2d(ImgList2D L, Work w)
             const int wi = br * WPR + (bc >> 5);
             const uint32_t sm = WS[wi] & ((2u << (bc & 31)) - 1u);
             const uint32_t sc = sm ? uint32_t(bc & ~31) + hibit(sm) : WCS[wi];
-            GUARD(w, sc < uint32_t(TBW), 113, sc);
+            (void)GUARD(w, sc < uint32_t(TBW), 113, sc);
             const uint32_t rb = key_block(P[sw(uint32_t(br) * TBW + (sc & (TBW - 1)))] >> 12);
             const uint32_t bit = 1u << (rb & 31);
             const uint32_t old = atomicOr(&BF[rb >> 5], bit);
