@@ -195,7 +195,7 @@ cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persist
         if (e == cudaSuccess) e = r;
     };
     mark(0);
-    k_tile_local_3d<<<grid(w.n_tiles, 6), kT3LocalThreads, 0, s>>>(L, wk);
+    k_tile_local_3d<<<grid(w.n_tiles, kT3LocalPerSM), kT3LocalThreads, 0, s>>>(L, wk);
     keep(cudaGetLastError());
     mark(1);
     keep(launch_k(k_merge_3d, grid(w.n_tiles, 8), kT3MergeThreads, s, ov, L, wk));

@@ -31,6 +31,7 @@ __global__ void k_chunk_sums(Work w);
 constexpr int kPostThreads = 128;   // k_chunk_sums
 constexpr int kT3Threads = 256;
 constexpr int kT3LocalThreads = T3_TB0 * T3_TB1;   // k_tile_local_3d: one thread per block row
+constexpr int kT3LocalPerSM = 7;   // k_tile_local_3d: resident CTAs per SM (31 KB of shared memory each)
 constexpr int kT3MergeThreads = 128;   // k_merge_3d: 8 tiles in flight per SM
 constexpr int kScanThreads = 256;
 

@@ -140,7 +140,7 @@ __device__ __forceinline__ bool perim_pos3(int p, const TileGeo &g, int &f, int 
 namespace {
 
 constexpr int NT1 = kT3LocalThreads;   // threads of the tile-local kernel: one per block row
-constexpr int MQ1 = 1536;          // union-queue capacity (more are merged in place)
+constexpr int MQ1 = 1024;          // union-queue capacity (more are merged in place)
 static_assert(TB2 == 32, "a block row along d2 is one 32-bit word");
 static_assert(NBLK <= 4096, "run starts must fit 12 bits");
 
@@ -235,7 +235,7 @@ __device__ __forceinline__ void split16b(uint4 v, uint32_t K, bool hi, uint32_t 
 
 }  // namespace
 
-__global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
+__global__ void __launch_bounds__(NT1, kT3LocalPerSM) k_tile_local_3d(ImgList3D L, Work w)
 {
     grid_dep_release();   // the merge launch may take free SMs during this grid's last wave
     if (blockIdx.x == 0 && threadIdx.x == 0) {   // a new epoch for the segment scan of this run
@@ -246,10 +246,11 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
     __shared__ __align__(16) uint8_t M[NBLK];  // block masks
     __shared__ uint32_t CW[8][NT1];            // class words of every row
     __shared__ uint32_t WHZ[NT1], WS[NT1];     // joins along d2, run starts
-    __shared__ uint32_t RB[TX * TY * RBW];
     __shared__ uint32_t BF[NBLK / 32];
     __shared__ uint32_t BP[NBLK / 32];
     __shared__ uint32_t MQ[MQ1];               // union queue: (block_a << 16) | block_b
+    static_assert(TX * TY * RBW <= MQ1, "the root bitmap fits the queue's memory");
+    uint32_t *const RB = MQ;                   // root bitmap (after the unions)
     __shared__ uint32_t mqn[4];                // queue counts of the union rounds
     __shared__ uint32_t tmp[NT1 / 32 + 1];
     __shared__ uint32_t qslot;
@@ -266,7 +267,6 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
         const bool hi = im.thr >= 128;
         const int64_t rs0 = int64_t(im.d1) * im.d2;   // stride of d0 in voxels
 
-        for (int i = tid; i < TX * TY * RBW; i += NT1) RB[i] = 0;
         BF[tid] = 0;
         if (tid < 4) mqn[tid] = 0;
 
@@ -467,6 +467,9 @@ __global__ void __launch_bounds__(NT1, 6) k_tile_local_3d(ImgList3D L, Work w)
             }
         }
 
+        // The root bitmap lives in the queue's memory from here on (the unions are done).
+        for (int i = tid; i < TX * TY * RBW; i += NT1) RB[i] = 0;
+        __syncthreads();
         // Phase C: every run start of this row is pointed straight at its root (a read-only walk,
         // then the root's entry stored in the start's own entry, as in 2D); roots mark their first
         // voxel.
