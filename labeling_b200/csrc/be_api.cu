@@ -198,7 +198,7 @@ cudaError_t launch_uf3d(const ImgList3D &L, const Work &w, int sms, bool persist
     k_tile_local_3d<<<grid(w.n_tiles, kT3LocalPerSM), kT3LocalThreads, 0, s>>>(L, wk);
     keep(cudaGetLastError());
     mark(1);
-    keep(launch_k(k_merge_3d, grid(w.n_tiles, 8), kT3MergeThreads, s, ov, L, wk));
+    keep(launch_k(k_merge_3d, grid(w.n_tiles, kT3MergePerSM), kT3MergeThreads, s, ov, L, wk));
     mark(2);
     keep(launch_k(k_scan_link_3d, grid(int64_t(w.n_chunks) + w.n_tiles, 8), kScanThreads, s, ov, L, wk));
     mark(3);

@@ -32,7 +32,8 @@ constexpr int kPostThreads = 128;   // k_chunk_sums
 constexpr int kT3Threads = 256;
 constexpr int kT3LocalThreads = T3_TB0 * T3_TB1;   // k_tile_local_3d: one thread per block row
 constexpr int kT3LocalPerSM = 7;   // k_tile_local_3d: resident CTAs per SM (31 KB of shared memory each)
-constexpr int kT3MergeThreads = 128;   // k_merge_3d: 8 tiles in flight per SM
+constexpr int kT3MergeThreads = 128;   // k_merge_3d threads
+constexpr int kT3MergePerSM = 9;       // k_merge_3d: tiles in flight per SM (23.5 KB of shared memory each)
 constexpr int kScanThreads = 256;
 
 }  // namespace be

@@ -644,7 +644,7 @@ __device__ void gunion3d(const Img3D &im, Work &w, uint32_t a, uint32_t b)
 // dense volume that crosses a face with one component in hundreds of blocks costs a handful of
 // global unions.
 constexpr int kGQ3 = 256;    // queued global unions per tile (more are done at once)
-constexpr int kPL3 = 1152;   // listed face pairs per tile (more are checked where they are found)
+constexpr int kPL3 = 576;    // listed face pairs per tile (more are checked where they are found)
 constexpr int PF0 = (TB1 + 2) * (TB2 + 2);   // staged entries across the +d0 face
 constexpr int PF1 = (TB0 + 2) * (TB2 + 2);   // +d1
 constexpr int PF2 = (TB0 + 2) * (TB1 + 2);   // +d2
@@ -734,7 +734,7 @@ __device__ __forceinline__ bool staged_pos(int e, int &iu, int &iv)
     return true;
 }
 
-__global__ void __launch_bounds__(kT3MergeThreads, 8) k_merge_3d(ImgList3D L, Work w)
+__global__ void __launch_bounds__(kT3MergeThreads, kT3MergePerSM) k_merge_3d(ImgList3D L, Work w)
 {
     grid_dep_wait();
     grid_dep_release();
