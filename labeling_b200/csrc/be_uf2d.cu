@@ -7,15 +7,18 @@
 //
 //   k_tile_local_2d   one CTA per 64x256-pixel tile: 16-byte coalesced loads, 2x2 block masks,
 //                     runs of blocks and their links by bit operations; each run's first link
-//                     becomes its parent by a plain store (a forest, flattened by pointer jumping),
-//                     the other links are atomicMin unions in shared memory (smaller key wins);
+//                     becomes its parent by a plain store (a forest), the other links are
+//                     atomicMin unions in shared memory (smaller key wins), then every run start
+//                     walks to its root;
 //                     write one uint16 per block = (mask << 12) | tile-local root block; count
 //                     roots per segment; mark each component's first pixel in the tile's root
 //                     bitmap; export border components as nodes.
-//   k_merge_2d        unions nodes across tile borders (global union-find, smaller key wins);
-//                     every root that gets linked leaves its segment count and its root bitmap.
+//   k_merge_2d        unions nodes across tile borders (global union-find after Rem's
+//                     algorithm, smaller key wins); every root that gets linked leaves its segment
+//                     count and its root bitmap.
 //   k_scan_flatten_2d single-pass exclusive scan of the segment counts (be_scan.cuh) and, in
-//                     the same launch, every linked node pointed straight at its global root.
+//                     the same launch, every linked node pointed at its global root (pointer
+//                     jumping).
 //   k_tile_write_2d   one CTA per tile: resolves each block's canonical label and writes the int32
 //                     labels with 16-byte stores.
 //

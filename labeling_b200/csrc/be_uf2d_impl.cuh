@@ -734,8 +734,8 @@ __global__ void __launch_bounds__(K2_NT, K2_PER_SM) k_merge_2d(ImgList2D L, Work
 // ---------------------------------------------------------------------------------------------
 // Segment scan and node flatten, one launch: items below n_chunks scan a chunk of segment counts
 // (single pass, look-back); the others point every linked node of one tile straight at its global
-// root (all unions are done, so every writer stores the same final root), so that the label
-// writes find each root in one step however long the merge's chains grew.
+// root (flatten_tile_nodes: all unions are done; the nodes of all tiles jump at once), so that the
+// label writes find each root in one step however long the merge's chains grew.
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kScanThreads) k_scan_flatten_2d(Work w)
 {

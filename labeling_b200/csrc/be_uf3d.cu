@@ -5,14 +5,16 @@
 // four-launch structure as the 2D pipeline (be_uf2d_impl.cuh):
 //
 //   k_tile_local_3d   one CTA per 16 x 32 x 64-voxel tile (8 x 16 x 32 blocks): 16-byte loads,
-//                     8-bit block masks, shared-memory union-find over the 13 preceding
-//                     neighbours, flatten, per-component first-voxel key (atomicMin), one uint32
-//                     per block, segment root counts, a per-tile bitmap of component first
-//                     voxels, border components exported as nodes.
+//                     voxel-class words per block row, runs along d2 and their links to the four
+//                     preceding rows by bit operations, a shared-memory union-find over runs (the
+//                     run of the component's first voxel stays the root), one uint32 per block,
+//                     segment root counts, a per-tile bitmap of component first voxels, border
+//                     components exported as nodes.
 //   k_merge_3d        global union-find over nodes across the +d0 / +d1 / +d2 tile faces; a root
 //                     linked under another leaves its segment count and its tile's bitmap.
-//   k_scan_flatten_3d exclusive scan of the segment counts (single pass, look-back) and
-//                     flattening of the linked nodes, one launch.
+//   k_scan_link_3d    exclusive scan of the segment counts (single pass, look-back) and, in the
+//                     same launch, every linked node pointed at its global root with the segment
+//                     and in-segment rank of that root's first voxel resolved.
 //   k_tile_write_3d   resolves canonical labels (segment prefix + rank in the bitmap row) and
 //                     writes int32 voxels with 16-byte stores.
 //
@@ -26,8 +28,9 @@
 // 0 of A and offset 1 of B can touch, along an axis with d = 0 every offset can.  This is the
 // predicate the reference evaluates voxel by voxel with TEST_CONN1/2/4 (LabelingAlgs.cl:770-856).
 //
-// Within a tile the union keeps the smaller block index as the root; the component's key (its
-// smallest first-voxel index) is then gathered per root with atomicMin.
+// Within a tile the union-find entries carry the slot (b0, i, b1, j, b2) of a run's first voxel,
+// whose order is the raster order of first voxels, and the atomicMin union keeps the smaller slot as
+// the root: the root run of a component holds its first voxel.
 #include "be_common.cuh"
 #include "be_kernels.h"
 #include "be_scan.cuh"
