@@ -111,3 +111,64 @@ def test_filtered_pairs_are_implied_by_queued_ones(seed):
     run([pair_thread(P, i, n_own + k, g_own[i], sid[k], queued) for i, k in pairs], rng)
     for i, k in pairs:
         assert connected(queued, g_own[i], sid[k]), (i, k, sid[k], queued)
+
+
+def border_thread(P, p, own, cb, sid, rs, n_own_slots, queued):
+    """One border position of k_merge_2d's pair loop: staged neighbour p + d for each connected
+    offset d; skipped when the node was just paired by this position (lastB) or when the position
+    before, of the same own node, touches the same staged run; else the local filter decides."""
+    ja = own[p]
+    if ja < 0:
+        return
+    prev_cb = cb[p - 1] if p > 0 and own[p - 1] == ja else 0
+    last_b = None
+    for d in (-1, 0, 1):
+        if not (cb[p] >> (d + 1)) & 1:
+            continue
+        i = p + d
+        n_b = sid[i]
+        if n_b == last_b:
+            continue
+        if any((prev_cb >> (dp + 1)) & 1 and rs[p - 1 + dp] == rs[i] for dp in (-1, 0, 1)):
+            continue
+        res = []
+        yield from smerge_joined(P, ja, n_own_slots + rs[i], res)
+        if res[0]:
+            queued.append((1000 + ja, n_b))
+        last_b = n_b
+
+
+@pytest.mark.parametrize("seed", range(300))
+def test_border_pairs_with_the_previous_position_rule(seed):
+    """Every connected (own node, staged node) pair along a border is implied by the queued pairs
+    when pairs covered by the previous position are skipped."""
+    rng = random.Random(seed + 77)
+    n_pos = rng.randint(2, 40)
+    n_own_nodes, n_nodes = rng.randint(1, 6), rng.randint(1, 8)
+    # own nodes along the border in runs (-1: empty), staged node ids in runs, staged index = position
+    own, sid = [], []
+    while len(own) < n_pos:
+        own += [rng.choice([-1] + list(range(n_own_nodes)))] * rng.randint(1, 5)
+    while len(sid) < n_pos + 1:
+        sid += [rng.randrange(n_nodes)] * rng.randint(1, 5)
+    own, sid = own[:n_pos], sid[:n_pos + 1]
+    rs = [0] * len(sid)                              # staged run starts (same id, consecutive)
+    for i in range(1, len(sid)):
+        rs[i] = rs[i - 1] if sid[i] == sid[i - 1] else i
+    cb = []
+    for p in range(n_pos):
+        m = 0
+        for d in (-1, 0, 1):
+            i = p + d
+            if own[p] >= 0 and 0 <= i < len(sid) and rng.random() < 0.6:
+                m |= 1 << (d + 1)
+        cb.append(m)
+    P = list(range(n_own_nodes + len(sid)))
+    for i in range(len(sid)):
+        P[n_own_nodes + i] = n_own_nodes + rs[i]
+    queued = []
+    run([border_thread(P, p, own, cb, sid, rs, n_own_nodes, queued) for p in range(n_pos)], rng)
+    for p in range(n_pos):
+        for d in (-1, 0, 1):
+            if (cb[p] >> (d + 1)) & 1:
+                assert connected(queued, 1000 + own[p], sid[p + d]), (p, d)
